@@ -1,0 +1,346 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the cpsFDTD time-stepping loop on B200.
+
+Workload (default): the dispersive-scattering deck -- 256^3 cells, dx 5 nm,
+CPML 12, TF/SF Gaussian beam (inset 20, 550 nm, theta 30, phi 45, pulse
+tau 4 fs), 4x4x4 Drude-Lorentz spheres (r 15, pitch 40), six planar ports with
+64-frequency FP64 DFTs; FP32 fields, fused path.  One bench step = one whole
+job of --job-steps time steps (default 4000) from a reset state, ports flushed.
+Synthetic geometry from the seeded deck generator; no dataset.
+
+Metric: Gcell-upd/s = cells x time steps / time, whole job, all ranks.
+  value  : device-timed (CUDA events on the grid's stream), inputs in HBM
+  e2e    : through the C ABI from host buffers: grid setup from the deck and
+           the host ID grid, the run, and the port spectra read back to host
+  roofline: the E sweep (dominant kernel) algorithmic bytes / its mean
+           event-timed duration, against the measured HBM copy bandwidth
+  cpu_baseline: the reference's own OpenMP code (oracle/_ref/ref_bench; its
+           3-D Drude-Lorentz from the oracle restatement) on the same deck
+Multi-GPU: one replica job per rank (the path does not shard), weak scaling.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="grid edge (cells)")
+    ap.add_argument("--job-steps", type=int, default=4000)
+    ap.add_argument("--e2e-steps", type=int, default=2, help="end-to-end jobs to time")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-steps", type=int, default=3, help="time steps in the CPU baseline sample")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="cps_clk_", suffix=".csv")
+        os.close(fd)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                smax.append(float(f[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(n, job_steps):
+    from cpsfdtd_b200 import decks
+    return decks.config2(n=n, steps=job_steps, nfreq=64)
+
+
+def sweep_bytes(dk, ndl, prec_bytes=4):
+    """Algorithmic bytes of one H sweep and one E sweep (FP32): each field word
+    read and written once, 1 B material ID, CPML psi (2 words read+write per
+    slab cell per sweep), Drude-Lorentz state (3 x (nD + 2 nL + 1) words read
+    + write per ID-2 cell).  Neighbour re-reads are not counted."""
+    nx, ny, nz, s = dk.nx, dk.ny, dk.nz, prec_bytes
+    np_ = dk.pml["npml"][0] if dk.pml else 0
+    h_cells = nx * ny * nz
+    e_cells = (nx - 1) * (ny - 1) * (nz - 1)
+    h_slab = 2 * np_ * (ny * nz + nx * nz + nx * ny)
+    e_slab = 2 * np_ * ((ny - 1) * (nz - 1) + (nx - 1) * (nz - 1) + (nx - 1) * (ny - 1))
+    psi = 2 * 2 * s
+    h = h_cells * (9 * s + 1) + h_slab * psi
+    stride = len(dk.dl["fD"]) + 2 * len(dk.dl["fL"]) + 1 if dk.dl else 0
+    e = e_cells * (9 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s
+    return h, e
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local, dist
+
+
+def cpu_baseline(dk, steps):
+    """The reference's own code on the same deck, bounded sample on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    if os.path.exists(oracle.REF_BENCH):
+        r = oracle.ref_bench(dk, 1, steps, threads=threads)
+        kind = "reference"
+        sample = (f"{dk.nx}^3 deck, {steps} time steps after 1 warm-up, reference BasicFDTD/CPML/TF_SF/Ports "
+                  f"(OpenMP) + 3-D Drude-Lorentz from the oracle restatement")
+    else:
+        o = oracle.Oracle.from_deck(dk, _ids(dk))
+        oracle.Oracle.threads(threads)
+        o.step(1)
+        t0 = time.perf_counter()
+        o.step(steps)
+        r = {"cells": dk.cells, "steps": steps, "seconds": time.perf_counter() - t0, "threads": threads}
+        kind = "port"
+        sample = f"{dk.nx}^3 deck, {steps} time steps after 1 warm-up, oracle restatement (OpenMP)"
+    gcell = r["cells"] * r["steps"] / r["seconds"] / 1e9
+    return {"value": gcell, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample}
+
+
+_IDS = {}
+
+
+def _ids(dk):
+    import cpsfdtd_b200 as cps
+    key = (dk.nx, dk.ny, dk.nz)
+    if key not in _IDS:
+        _IDS[key] = dk.ids if dk.ids is not None else cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    return _IDS[key]
+
+
+def run_reference(args):
+    world, rank, local, dist = dist_setup()
+    if rank != 0:
+        return
+    dk = workload(args.n, args.job_steps)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    threads = os.cpu_count() or 1
+    if os.path.exists(oracle.REF_BENCH):
+        r = oracle.ref_bench(dk, args.warmup, args.steps, threads=threads)
+        kind, what = "reference", "reference BasicFDTD/CPML/TF_SF/Ports (OpenMP) + 3-D Drude-Lorentz from the oracle restatement"
+    else:
+        o = oracle.Oracle.from_deck(dk, _ids(dk))
+        oracle.Oracle.threads(threads)
+        o.step(args.warmup)
+        t0 = time.perf_counter()
+        o.step(args.steps)
+        r = {"cells": dk.cells, "steps": args.steps, "seconds": time.perf_counter() - t0, "threads": threads}
+        kind, what = "port", "oracle restatement (OpenMP)"
+    v = r["cells"] * r["steps"] / r["seconds"] / 1e9
+    sample = f"{dk.nx}^3 dispersive-scattering deck, {args.steps} time steps after {args.warmup} warm-up, {what}"
+    line = {"metric": "Gcell-upd/s", "value": v, "unit": "Gcell-upd/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded deck generator)",
+            "config": {"workload": f"dispersive scattering {dk.nx}^3 (1 bench step = 1 time step on CPU)"},
+            "cpu_baseline": {"value": v, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    world, rank, local, dist = dist_setup()
+    import cpsfdtd_b200 as cps
+    torch.cuda.set_device(local)
+    dk = workload(args.n, args.job_steps)
+    ids = _ids(dk)
+    pts = [cps.port_points(dk, p) for p in dk.ports]
+    g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts, device=local)
+    stream = torch.cuda.ExternalStream(g.stream(), device=local)
+
+    def job(grid):
+        grid.reset(dk.n0)
+        grid.step(dk.nsteps, cps.FUSED)
+        grid.flush_ports()
+
+    for _ in range(args.warmup):
+        job(g)
+    g.sync()
+    launches0 = g.launches()
+    g.set_timing(8)
+    clocks = Clocks(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        job(g)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    launches = g.launches() - launches0
+    h_ms, e_ms, nsamp = g.timing()
+    g.set_timing(0)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = dk.cells
+    total = cells * dk.nsteps * args.steps * world
+    value = total / (ms / 1e3) / 1e9
+
+    # roofline of the dominant kernel (E sweep)
+    P, src = peaks()
+    ndl = 0
+    from cpsfdtd_b200 import decks
+    ndl = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_DISPERSIVE).sum())
+    hb, eb = sweep_bytes(dk, ndl)
+    dom_ms, dom_bytes, dom = (e_ms, eb, "E sweep") if e_ms >= h_ms else (h_ms, hb, "H sweep")
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / P["hbm_gbs"], "peak_source": src, "traffic": None,
+            "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms, "samples": nsamp,
+            "h_sweep_ms": h_ms, "e_sweep_ms": e_ms,
+            "step_bytes_per_cell": (hb + eb) / cells,
+            "step_frac_at_50B": value / world * 50 / P["hbm_gbs"]}
+    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tr):
+        try:
+            roof["traffic"] = json.load(open(tr)).get("e_sweep_bytes_per_launch")
+        except (ValueError, OSError):
+            pass
+
+    # end to end through the C ABI from host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned_ids = torch.from_numpy(np.ascontiguousarray(ids)).pin_memory()
+        outs = []
+        h2d = d2h = 0
+        for p in dk.ports:
+            nc = bin(p.dft_mask).count("1")
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            gg = cps.Grid.from_deck(dk, cps.FP32, ids=pinned_ids.numpy(), port_points_list=pts, device=local)
+            gg.step(dk.nsteps, cps.FUSED)
+            outs = [gg.port_dft(n) for n in range(len(dk.ports))]
+            gg.close()
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([t_e2e], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        h2d = ids.nbytes + sum(p.nbytes for p in pts) + sum(len(w) * 8 for *_, w in dk.sources)
+        d2h = sum(o.nbytes for o in outs)
+        e2e = {"value": cells * dk.nsteps * args.e2e_steps * world / t_e2e / 1e9, "unit": "Gcell-upd/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(workload(args.n, args.job_steps), args.cpu_steps)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {ex}"}
+    if rank == 0:
+        line = {"metric": "Gcell-upd/s", "value": value, "unit": "Gcell-upd/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic (seeded deck generator)",
+                "config": {"workload": f"dispersive scattering {dk.nx}^3, Drude-Lorentz 4x4x4 spheres, CPML "
+                                       f"{dk.pml['npml'][0]}, TF/SF Gaussian beam, 6 ports x 64-freq FP64 DFT; "
+                                       f"1 bench step = 1 job of {dk.nsteps} time steps",
+                           "grid": [dk.nx, dk.ny, dk.nz], "time_steps_per_job": dk.nsteps,
+                           "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
+                           "l2": "inputs larger than L2 (fields 0.40 GB per grid)", "parallelism": f"replicas x{world}"},
+                "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
+                "e2e": e2e, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

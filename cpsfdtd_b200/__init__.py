@@ -1,0 +1,377 @@
+"""cpsfdtd_b200 -- B200-native time-stepping engine for cpsFDTD workloads.
+
+This module is a thin ctypes binding of ``libcpsfdtd.so`` (the C ABI declared
+in ``include/cps_capi.h``).  All compute runs in the CUDA kernels of that
+library; there is no CPU fallback: importing works without a GPU, but
+creating a :class:`Grid` without the built library or without a CUDA device
+raises.
+
+``Grid.from_deck(deck)`` sets up one simulation from a
+:class:`cpsfdtd_b200.decks.Deck` the same way the reference's constructors
+do (Structure, CPML, Drude_Lorentz, FourLevelLaser, TF_SF, ports).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+__all__ = ["Grid", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcpsfdtd.so")
+
+FP64, FP32 = 0, 1
+PLAIN, FUSED = 0, 1
+MAX_POLES = 8
+
+_lib = None
+
+
+class CpsError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"cps error {code}: {msg}")
+        self.code = code
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double), ("dt", C.c_double),
+                ("precision", C.c_int32), ("device", C.c_int32)]
+
+
+class PmlParams(C.Structure):
+    _fields_ = [("npml", C.c_int32 * 6), ("m", C.c_double), ("malp", C.c_double), ("kapmax", C.c_double),
+                ("sig_ratio", C.c_double), ("alpmax", C.c_double)]
+
+
+class DlParams(C.Structure):
+    _fields_ = [("sigma", C.c_double), ("epsInf", C.c_double), ("nD", C.c_int32), ("nL", C.c_int32),
+                ("fD", C.c_double * MAX_POLES), ("gD", C.c_double * MAX_POLES),
+                ("fL", C.c_double * MAX_POLES), ("dL", C.c_double * MAX_POLES), ("depsL", C.c_double * MAX_POLES),
+                ("literal", C.c_int32)]
+
+
+class GainParams(C.Structure):
+    _fields_ = [("gain_id", C.c_int32), ("lambda_a", C.c_double), ("lambda_b", C.c_double),
+                ("gamma_a", C.c_double), ("gamma_b", C.c_double), ("t30", C.c_double), ("t32", C.c_double),
+                ("t21", C.c_double), ("t10", C.c_double), ("N_0", C.c_double), ("pump_rate", C.c_double)]
+
+
+class TfsfParams(C.Structure):
+    _fields_ = [("lambda_", C.c_double), ("dlambda", C.c_double), ("w0", C.c_double), ("z0", C.c_double),
+                ("i0", C.c_int32), ("j0", C.c_int32), ("k0", C.c_int32),
+                ("theta_deg", C.c_double), ("phi_deg", C.c_double), ("E0", C.c_double), ("psi_deg", C.c_double),
+                ("n", C.c_int32 * 6), ("Nt", C.c_int32), ("cwmode", C.c_int32)]
+
+
+class Shape(C.Structure):
+    _fields_ = [("type", C.c_int32), ("material_index", C.c_int32), ("theta", C.c_double), ("phi", C.c_double),
+                ("psi", C.c_double), ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double),
+                ("a", C.c_double), ("b", C.c_double), ("c", C.c_double)]
+
+
+SHAPE_TYPES = {"cuboid": 0, "ellipsoid": 1, "cylinder": 2, "multi": 3}
+
+
+def lib():
+    """Load libcpsfdtd.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m cpsfdtd_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        P, I32, I64, D, U32 = C.c_void_p, C.c_int32, C.c_int64, C.c_double, C.c_uint32
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+        sigs = {
+            "cps_last_error": ([], C.c_char_p), "cps_version": ([], C.c_char_p),
+            "cps_courant_dt": ([D, D, D], D),
+            "cps_grid_create": ([C.POINTER(GridDesc), C.POINTER(P)], I32),
+            "cps_grid_destroy": ([P], I32), "cps_grid_info": ([P, C.POINTER(GridDesc)], I32),
+            "cps_grid_bytes": ([P, C.POINTER(I64)], I32),
+            "cps_grid_set_stream": ([P, P], I32), "cps_grid_get_stream": ([P, C.POINTER(P)], I32),
+            "cps_synchronize": ([P], I32),
+            "cps_grid_set_media": ([P, I32, dp, dp, dp, dp], I32),
+            "cps_grid_upload_ids": ([P, P], I32), "cps_grid_download_ids": ([P, P], I32),
+            "cps_mesh_rasterize": ([I32, I32, I32, D, D, D, I32, C.POINTER(Shape), P, I32], I32),
+            "cps_pml_init": ([P, C.POINTER(PmlParams)], I32),
+            "cps_dl_init": ([P, C.POINTER(DlParams)], I32),
+            "cps_gain_init": ([P, C.POINTER(GainParams)], I32),
+            "cps_tfsf_init": ([P, C.POINTER(TfsfParams)], I32),
+            "cps_tfsf_set_tables": ([P, I32, dp, dp], I32), "cps_tfsf_get_tables": ([P, I32, dp, dp], I32),
+            "cps_source_add": ([P, I32, I32, I32, I32, dp, I32], I32),
+            "cps_port_points_plain": ([I32, I32, I32, D, D, D, C.c_char, D, D, D, D, D, ip, ip], I32),
+            "cps_port_points_spherical": ([I32, I32, I32, D, D, D, D, D, D, D, D, D, D, D, ip, ip], I32),
+            "cps_port_add": ([P, I32, ip, ip], I32),
+            "cps_port_set_dft": ([P, I32, I32, dp, U32], I32),
+            "cps_port_read": ([P, I32, dp], I32), "cps_port_dft_read": ([P, I32, dp], I32),
+            "cps_port_flux": ([P, I32, C.c_char, dp], I32),
+            "cps_grid_set_step": ([P, I64], I32), "cps_grid_get_step": ([P, C.POINTER(I64)], I32),
+            "cps_step": ([P, I32, I32], I32),
+            "cps_op_h_bulk": ([P], I32), "cps_op_e_bulk": ([P], I32), "cps_op_h_pml": ([P], I32),
+            "cps_op_e_pml": ([P], I32), "cps_op_dl": ([P], I32), "cps_op_gain_polarization": ([P], I32),
+            "cps_op_gain_efield": ([P], I32), "cps_op_gain_populations": ([P], I32),
+            "cps_op_tfsf_h": ([P, I32, U32], I32), "cps_op_tfsf_e": ([P, I32, U32], I32),
+            "cps_op_sources": ([P, I32], I32), "cps_op_port_sample": ([P, I32, I32], I32),
+            "cps_field_download": ([P, I32, dp], I32), "cps_field_upload": ([P, I32, dp], I32),
+            "cps_field_download_f32": ([P, I32, C.POINTER(C.c_float)], I32),
+            "cps_grid_reset": ([P, I64], I32), "cps_grid_check_finite": ([P, C.POINTER(I64)], I32),
+            "cps_gain_populations": ([P, dp, C.POINTER(I64)], I32),
+            "cps_grid_launch_count": ([P, C.POINTER(I64)], I32),
+            "cps_ports_flush": ([P], I32), "cps_grid_set_timing": ([P, I32], I32),
+            "cps_grid_timing": ([P, C.POINTER(D), C.POINTER(D), C.POINTER(I64)], I32),
+        }
+        for name, (args, res) in sigs.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(code):
+    if code != 0:
+        raise CpsError(code, lib().cps_last_error().decode())
+
+
+def _dp(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def rasterize(nx, ny, nz, dx, dy, dz, shapes) -> np.ndarray:
+    """ID grid [i][j][k] of structure.txt shapes, as Structure::generate_mesh."""
+    arr = (Shape * max(1, len(shapes)))()
+    for n, s in enumerate(shapes):
+        arr[n] = Shape(SHAPE_TYPES[s.type], s.mat, s.theta, s.phi, s.psi, s.x0, s.y0, s.z0, s.a, s.b, s.c)
+    ids = np.zeros((nx + 1, ny + 1, nz + 1), dtype=np.uint8)
+    _check(lib().cps_mesh_rasterize(nx, ny, nz, dx, dy, dz, len(shapes), arr, ids.ctypes.data, 0))
+    return ids
+
+
+def port_points(deck, port) -> np.ndarray:
+    """Point set [(i, j, k)] of a deck port, as the reference port constructors build it."""
+    L = lib()
+    q = port.params
+    cnt = C.c_int32(0)
+    if port.kind == "plain":
+        args = (deck.nx, deck.ny, deck.nz, deck.dx, deck.dy, deck.dz, q["dir"].encode(), q["position"],
+                q["w1"], q["w2"], q["h1"], q["h2"])
+        _check(L.cps_port_points_plain(*args, C.byref(cnt), None))
+        out = np.zeros((cnt.value, 3), dtype=np.int32)
+        _check(L.cps_port_points_plain(*args, C.byref(cnt), out.ctypes.data_as(C.POINTER(C.c_int32))))
+    else:
+        args = (deck.nx, deck.ny, deck.nz, deck.dx, deck.dy, deck.dz, q["r"], q["xc"], q["yc"], q["zc"],
+                q["theta1"], q["theta2"], q["phi1"], q["phi2"])
+        _check(L.cps_port_points_spherical(*args, C.byref(cnt), None))
+        out = np.zeros((cnt.value, 3), dtype=np.int32)
+        _check(L.cps_port_points_spherical(*args, C.byref(cnt), out.ctypes.data_as(C.POINTER(C.c_int32))))
+    return out
+
+
+class Grid:
+    """One simulation domain resident on one GPU."""
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, dt=0.0, precision=FP32, device=0):
+        self.L = lib()
+        self.h = C.c_void_p()
+        self.desc = GridDesc(nx, ny, nz, dx, dy, dz, dt, precision, device)
+        _check(self.L.cps_grid_create(C.byref(self.desc), C.byref(self.h)))
+        info = GridDesc()
+        _check(self.L.cps_grid_info(self.h, C.byref(info)))
+        self.dt = info.dt
+        self.shape3 = (nx + 1, ny + 1, nz + 1)
+        self.precision = precision
+        self.ports = []  # (npts, ncomp, nfreq)
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.cps_grid_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --------------------------------------------------------- setup
+    @classmethod
+    def from_deck(cls, dk, precision=FP32, ids: Optional[np.ndarray] = None, device=0, port_points_list=None):
+        g = cls(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.dt, precision, device)
+        g.set_media(dk.media)
+        if ids is None:
+            ids = dk.ids if dk.ids is not None else rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+        g.upload_ids(ids)
+        if dk.pml:
+            g.pml_init(dk.pml)
+        if dk.dl:
+            g.dl_init(dk.dl)
+        if dk.gain:
+            g.gain_init(dk.gain)
+        if dk.tfsf:
+            g.tfsf_init(dk.tfsf_abi())
+        for comp, i, j, k, wave in dk.sources:
+            g.source_add(comp, i, j, k, wave)
+        for n, p in enumerate(dk.ports):
+            pts = port_points_list[n] if port_points_list is not None else port_points(dk, p)
+            pid = g.port_add(pts)
+            if p.dft_freqs is not None:
+                g.port_set_dft(pid, p.dft_freqs, p.dft_mask)
+        g.set_step(dk.n0)
+        return g
+
+    def set_media(self, media):
+        m = np.array(media, dtype=np.float64).reshape(-1, 4)
+        cols = [_dp(m[:, c]) for c in range(4)]
+        _check(self.L.cps_grid_set_media(self.h, len(m), *[c[1] for c in cols]))
+
+    def upload_ids(self, ids):
+        ids = np.ascontiguousarray(ids, dtype=np.uint8)
+        assert ids.shape == self.shape3, (ids.shape, self.shape3)
+        _check(self.L.cps_grid_upload_ids(self.h, ids.ctypes.data))
+
+    def download_ids(self):
+        out = np.empty(self.shape3, dtype=np.uint8)
+        _check(self.L.cps_grid_download_ids(self.h, out.ctypes.data))
+        return out
+
+    def pml_init(self, p):
+        pp = PmlParams((C.c_int32 * 6)(*p["npml"]), p["m"], p["malp"], p["kapmax"], p["sig_ratio"], p["alpmax"])
+        _check(self.L.cps_pml_init(self.h, C.byref(pp)))
+
+    def dl_init(self, d):
+        z = [0.0] * MAX_POLES
+        def arr(v):
+            return (C.c_double * MAX_POLES)(*(list(v) + z)[:MAX_POLES])
+        pp = DlParams(d["sigma"], d["epsInf"], len(d["fD"]), len(d["fL"]), arr(d["fD"]), arr(d["gD"]),
+                      arr(d["fL"]), arr(d["dL"]), arr(d["depsL"]), int(d.get("literal", 0)))
+        _check(self.L.cps_dl_init(self.h, C.byref(pp)))
+
+    def gain_init(self, g):
+        pp = GainParams(int(g.get("gain_id", 5)), g["lambda_a"], g["lambda_b"], g["gamma_a"], g["gamma_b"],
+                        g["t30"], g["t32"], g["t21"], g["t10"], g["N_0"], g.get("pump", 0.0))
+        _check(self.L.cps_gain_init(self.h, C.byref(pp)))
+
+    def tfsf_init(self, t):
+        pp = TfsfParams(t["lambda_"], t["dlambda"], t["w0"], t["z0"], t["i0"], t["j0"], t["k0"], t["theta"],
+                        t["phi"], t["E0"], t["psi"], (C.c_int32 * 6)(*t["n6"]), t["Nt"], t["cwmode"])
+        _check(self.L.cps_tfsf_init(self.h, C.byref(pp)))
+        self.tfsf_Nt = t["Nt"]
+
+    def tfsf_tables(self):
+        n = self.tfsf_Nt + 1
+        e, h = np.empty(n), np.empty(n)
+        _check(self.L.cps_tfsf_get_tables(self.h, n, e.ctypes.data_as(C.POINTER(C.c_double)),
+                                          h.ctypes.data_as(C.POINTER(C.c_double))))
+        return e, h
+
+    def source_add(self, comp, i, j, k, wave):
+        w = _dp(wave)
+        _check(self.L.cps_source_add(self.h, comp, i, j, k, w[1], len(w[0])))
+
+    def port_add(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.int32).reshape(-1, 3)
+        pid = C.c_int32()
+        _check(self.L.cps_port_add(self.h, len(pts), pts.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(pid)))
+        self.ports.append([len(pts), 0, 0])
+        return pid.value
+
+    def port_set_dft(self, pid, freqs, mask=0x3F):
+        f = _dp(freqs)
+        _check(self.L.cps_port_set_dft(self.h, pid, len(f[0]), f[1], mask))
+        self.ports[pid][1] = bin(mask & 63).count("1")
+        self.ports[pid][2] = len(f[0])
+
+    # ---------------------------------------------------------- run
+    def set_step(self, n):
+        _check(self.L.cps_grid_set_step(self.h, n))
+
+    def get_step(self):
+        n = C.c_int64()
+        _check(self.L.cps_grid_get_step(self.h, C.byref(n)))
+        return n.value
+
+    def step(self, n=1, path=FUSED):
+        _check(self.L.cps_step(self.h, n, path))
+
+    def sync(self):
+        _check(self.L.cps_synchronize(self.h))
+
+    def reset(self, n0=1):
+        _check(self.L.cps_grid_reset(self.h, n0))
+
+    def op(self, name, *args):
+        _check(getattr(self.L, "cps_op_" + name)(self.h, *args))
+
+    # ------------------------------------------------------- access
+    def field(self, comp):
+        out = np.empty(self.shape3, dtype=np.float64)
+        _check(self.L.cps_field_download(self.h, comp, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def fields(self):
+        return [self.field(c) for c in range(6)]
+
+    def set_field(self, comp, a):
+        a, p = _dp(a)
+        assert a.shape == self.shape3
+        _check(self.L.cps_field_upload(self.h, comp, p))
+
+    def port_last(self, pid):
+        out = np.empty((self.ports[pid][0], 6))
+        _check(self.L.cps_port_read(self.h, pid, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def port_dft(self, pid, raw=False):
+        """DFT accumulators; raw=True gives the ABI layout [ncomp][nfreq][2][npts],
+        otherwise a [npts][ncomp][nfreq][2] view of it."""
+        npts, ncomp, nfreq = self.ports[pid]
+        out = np.empty((ncomp, nfreq, 2, npts))
+        _check(self.L.cps_port_dft_read(self.h, pid, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out if raw else out.transpose(3, 0, 1, 2)
+
+    def port_flux(self, pid, normal):
+        out = np.empty(self.ports[pid][2])
+        _check(self.L.cps_port_flux(self.h, pid, normal.encode(), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def nonfinite(self):
+        n = C.c_int64()
+        _check(self.L.cps_grid_check_finite(self.h, C.byref(n)))
+        return n.value
+
+    def populations(self):
+        n = C.c_int64()
+        _check(self.L.cps_gain_populations(self.h, None, C.byref(n)))
+        out = np.empty((n.value, 4))
+        _check(self.L.cps_gain_populations(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)))
+        return out
+
+    def device_bytes(self):
+        n = C.c_int64()
+        _check(self.L.cps_grid_bytes(self.h, C.byref(n)))
+        return n.value
+
+    def launches(self):
+        n = C.c_int64()
+        _check(self.L.cps_grid_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def flush_ports(self):
+        _check(self.L.cps_ports_flush(self.h))
+
+    def set_timing(self, stride):
+        _check(self.L.cps_grid_set_timing(self.h, stride))
+
+    def timing(self):
+        h, e, n = C.c_double(), C.c_double(), C.c_int64()
+        _check(self.L.cps_grid_timing(self.h, C.byref(h), C.byref(e), C.byref(n)))
+        return h.value, e.value, n.value
+
+    def stream(self):
+        p = C.c_void_p()
+        _check(self.L.cps_grid_get_stream(self.h, C.byref(p)))
+        return p.value

@@ -1,0 +1,1482 @@
+// capi.cpp -- the C ABI of include/cps_capi.h: grid objects, host FP64
+// coefficient builders (restating Structure.cpp:309-359, CPML.cpp:139-527,
+// Drude_Lorentz.cpp:65-108, FourLevelLaser.cpp:96-105/202-209,
+// TF_SF.cpp:98-955), device allocation, and the step driver.
+//
+// Built without FMA contraction (host code), so coefficient values equal the
+// oracle's bit for bit.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cps_internal.h"
+
+namespace cps {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+}  // namespace cps
+
+using namespace cps;
+
+extern "C" const char *cps_last_error(void) { return g_last_error.c_str(); }
+extern "C" const char *cps_version(void) { return "cpsfdtd-b200 0.1 (sm_100a)"; }
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) {                                                                   \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                         \
+            return e_ == cudaErrorMemoryAllocation ? CPS_E_NOMEM : CPS_E_CUDA;                     \
+        }                                                                                          \
+    } while (0)
+
+#define REQUIRE(cond, code, msg)                                                                   \
+    do {                                                                                           \
+        if (!(cond)) {                                                                             \
+            set_error(msg);                                                                        \
+            return code;                                                                           \
+        }                                                                                          \
+    } while (0)
+
+namespace {
+
+struct PortState {
+    int npts = 0;
+    std::vector<int32_t> ijk;
+    int64_t *d_idx = nullptr;
+    void *d_ring = nullptr;  // [slots][6][npts] of T
+    int slots = 1;
+    int fill = 0;            // samples in the ring not yet folded into the DFT
+    int64_t ring_n0 = 0;     // step of ring slot 0
+    int last_slot = -1;
+    int nfreq = 0;
+    uint32_t mask = 0;
+    int ncomp = 0;
+    int comps[6] = {0, 0, 0, 0, 0, 0};
+    int32_t *d_comps = nullptr;
+    double *d_omega = nullptr;
+    double *d_acc = nullptr;  // [ncomp][nfreq][2][npts]
+};
+
+struct Src {
+    int comp;
+    int64_t idx;
+    std::vector<double> wave;
+};
+
+}  // namespace
+
+struct cps_grid {
+    cps_grid_desc desc{};
+    bool fp32 = false;
+    size_t esz = 8;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Dims d{};
+    int64_t elems = 0;  // device elements per field array
+    void *F[6] = {};
+    uint8_t *d_id = nullptr;
+    std::vector<uint8_t> ids_dev;  // host copy in device order
+    bool ids_set = false;
+    int nmedia = 0;
+    double aE[256] = {}, bE[256] = {}, aH[256] = {}, bH[256] = {};
+    void *d_media = nullptr;  // aE bE aH bH, 256 each, of T
+    std::vector<double> st[12];
+    void *d_st = nullptr;
+    // CPML
+    bool pml_on = false;
+    cps_pml_params pml{};
+    std::vector<double> pbE[6], pcE[6], pbH[6], pcH[6];
+    void *d_pcoef = nullptr;
+    void *d_q[6][4] = {};
+    double cpmlE = 0, cpmlH = 0;
+    // Drude-Lorentz
+    bool dl_on = false;
+    DlCoef<double> dlc{};
+    int64_t dl_n = 0;
+    int64_t *d_dl_cell = nullptr;
+    int32_t *d_dl_seg = nullptr;
+    void *d_dl_state = nullptr;
+    // gain
+    bool gain_on = false;
+    GainCoef gc{};
+    int gain_id = 5;
+    int64_t g_n = 0;
+    int64_t *d_g_cell = nullptr;
+    int32_t *d_g_seg = nullptr;
+    void *d_g_state = nullptr;
+    // TF/SF
+    bool tfsf_on = false;
+    cps_tfsf_params tp{};
+    std::vector<double> einc, hinc;
+    void *d_einc = nullptr, *d_hinc = nullptr;
+    InjTarget *d_tg[2] = {nullptr, nullptr};   // 0: E targets, 1: H targets
+    InjContrib *d_ct[2] = {nullptr, nullptr};
+    int ntg[2] = {0, 0};
+    // sources
+    std::vector<Src> src;
+    int64_t *d_src_idx = nullptr;
+    int32_t *d_src_comp = nullptr, *d_src_off = nullptr, *d_src_len = nullptr;
+    double *d_src_wave = nullptr;
+    bool src_dirty = false;
+    // ports
+    std::vector<PortState> ports;
+    double *d_phasor = nullptr;
+    size_t phasor_cap = 0;
+    // misc
+    int64_t step = 1;
+    int64_t launches = 0;
+    FusedShape shape{8, 32};
+    double *d_conv = nullptr;
+    unsigned long long *d_counter = nullptr;
+    // sweep timing samples: events (start, after H sweep, after E sweep)
+    int timing_stride = 0;
+    std::vector<cudaEvent_t> ev;
+    int ev_used = 0;
+    std::vector<std::pair<void *, size_t>> owned;  // every device allocation and its size
+};
+
+namespace {
+
+cps_status dalloc(cps_grid *g, void **p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+        cudaGetLastError();
+        return CPS_E_NOMEM;
+    }
+    g->owned.push_back({*p, bytes});
+    e = cudaMemsetAsync(*p, 0, bytes, g->stream);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return CPS_E_CUDA; }
+    return CPS_OK;
+}
+
+void dfree(cps_grid *g, void *p)
+{
+    if (!p) return;
+    for (auto it = g->owned.begin(); it != g->owned.end(); ++it)
+        if (it->first == p) { g->owned.erase(it); break; }
+    cudaFree(p);
+}
+
+template <typename T>
+cps_status upload_T(cps_grid *g, void *dst, const double *src, size_t n)
+{
+    std::vector<T> tmp(n);
+    for (size_t q = 0; q < n; ++q) tmp[q] = (T)src[q];
+    CK(cudaMemcpyAsync(dst, tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+cps_status upload_real(cps_grid *g, void *dst, const double *src, size_t n)
+{
+    return g->fp32 ? upload_T<float>(g, dst, src, n) : upload_T<double>(g, dst, src, n);
+}
+
+cps_status upload_raw(cps_grid *g, void *dst, const void *src, size_t bytes)
+{
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+const int kStretchLen(const cps_grid *g, int w)
+{
+    const int n[12] = {g->d.nz, g->d.nz, g->d.ny, g->d.ny, g->d.nx, g->d.nx,
+                       g->d.nz, g->d.nz, g->d.ny, g->d.ny, g->d.nx, g->d.nx};
+    return n[w];
+}
+
+// stretch arrays on the device: 12 arrays packed, each padded to 8 entries
+cps_status push_stretch(cps_grid *g)
+{
+    std::vector<double> all;
+    for (int w = 0; w < 12; ++w) {
+        all.insert(all.end(), g->st[w].begin(), g->st[w].end());
+        all.resize((all.size() + 7) / 8 * 8, 0.0);
+    }
+    if (!g->d_st) {
+        cps_status s = dalloc(g, &g->d_st, all.size() * g->esz);
+        if (s) return s;
+    }
+    return upload_real(g, g->d_st, all.data(), all.size());
+}
+
+template <typename T>
+StretchView<T> stretch_view(const cps_grid *g)
+{
+    StretchView<T> v;
+    const T *base = (const T *)g->d_st;
+    const T *a[12];
+    size_t off = 0;
+    for (int w = 0; w < 12; ++w) {
+        a[w] = base + off;
+        off += (size_t)(kStretchLen(g, w) + 7) / 8 * 8;
+    }
+    v.cExy = a[0]; v.cEyx = a[1]; v.cEzx = a[2]; v.cExz = a[3]; v.cEzy = a[4]; v.cEyz = a[5];
+    v.cHxy = a[6]; v.cHyx = a[7]; v.cHzx = a[8]; v.cHxz = a[9]; v.cHzy = a[10]; v.cHyz = a[11];
+    return v;
+}
+
+template <typename T>
+FieldView<T> field_view(const cps_grid *g)
+{
+    FieldView<T> f;
+    f.d = g->d;
+    f.Ex = (T *)g->F[0]; f.Ey = (T *)g->F[1]; f.Ez = (T *)g->F[2];
+    f.Hx = (T *)g->F[3]; f.Hy = (T *)g->F[4]; f.Hz = (T *)g->F[5];
+    f.id = g->d_id;
+    const T *m = (const T *)g->d_media;
+    f.aE = m; f.bE = m + 256; f.aH = m + 512; f.bH = m + 768;
+    f.s = stretch_view<T>(g);
+    return f;
+}
+
+template <typename T>
+PmlView<T> pml_view(const cps_grid *g)
+{
+    PmlView<T> p;
+    memset(&p, 0, sizeof(p));
+    p.on = g->pml_on;
+    if (!g->pml_on) return p;
+    const T *c = (const T *)g->d_pcoef;
+    size_t off = 0;
+    for (int f = 0; f < 6; ++f) {
+        p.np[f] = g->pml.npml[f];
+        const size_t n = (size_t)p.np[f] + 1;
+        p.bE[f] = c + off; off += n;
+        p.cE[f] = c + off; off += n;
+        p.bH[f] = c + off; off += n;
+        p.cH[f] = c + off; off += n;
+        p.qe[f][0] = (T *)g->d_q[f][0]; p.qe[f][1] = (T *)g->d_q[f][1];
+        p.qh[f][0] = (T *)g->d_q[f][2]; p.qh[f][1] = (T *)g->d_q[f][3];
+    }
+    p.cpmlE = (T)g->cpmlE;
+    p.cpmlH = (T)g->cpmlH;
+    return p;
+}
+
+template <typename T>
+DlView<T> dl_view(const cps_grid *g)
+{
+    DlView<T> v;
+    memset(&v, 0, sizeof(v));
+    v.on = g->dl_on;
+    if (!g->dl_on) return v;
+    v.ncell = g->dl_n; v.cell = g->d_dl_cell; v.seg = g->d_dl_seg; v.state = (T *)g->d_dl_state;
+    const DlCoef<double> &c = g->dlc;
+    v.c.nD = c.nD; v.c.nL = c.nL; v.c.stride = c.stride;
+    v.c.C1 = (T)c.C1; v.c.C2 = (T)c.C2; v.c.C3 = (T)c.C3; v.c.dt = (T)c.dt; v.c.inv2dt = (T)c.inv2dt;
+    for (int p = 0; p < kMaxPoles; ++p) {
+        v.c.kappa[p] = (T)c.kappa[p]; v.c.beta[p] = (T)c.beta[p]; v.c.C4[p] = (T)c.C4[p];
+        v.c.alpha[p] = (T)c.alpha[p]; v.c.xi[p] = (T)c.xi[p]; v.c.gammaL[p] = (T)c.gammaL[p];
+        v.c.C5[p] = (T)c.C5[p]; v.c.C6[p] = (T)c.C6[p];
+    }
+    return v;
+}
+
+template <typename T>
+GainView<T> gain_view(const cps_grid *g)
+{
+    GainView<T> v;
+    memset(&v, 0, sizeof(v));
+    v.on = g->gain_on;
+    if (!g->gain_on) return v;
+    v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg;
+    v.state = (T *)g->d_g_state; v.c = g->gc;
+    return v;
+}
+
+// ------------------------------------------------------------ CPML coefs
+
+// E-side grading, CPML.cpp:139-183
+void grade_e(std::vector<double> &kappa, std::vector<double> &b, std::vector<double> &c, bool first, int np,
+             double dt, double del, double m, double ma, double sigmax, double kapmax, double alpmax)
+{
+    std::vector<double> sigma(np + 1), alpha(np + 1);
+    kappa.assign(np + 1, 0); b.assign(np + 1, 0); c.assign(np + 1, 0);
+    for (int i = 1; i <= np + 1; ++i) {
+        double ps, pa;
+        if (first) {
+            ps = pow(((double)np + 1.0 - i) / ((double)np), m);
+            pa = pow(((double)i - 1.0) / ((double)np), ma);
+        } else {
+            ps = pow(((double)i - 1.0) / np, m);
+            pa = pow(((double)np + 1.0 - i) / np, ma);
+        }
+        sigma[i - 1] = sigmax * ps;
+        kappa[i - 1] = 1.0 + (kapmax - 1.0) * ps;
+        alpha[i - 1] = alpmax * pa;
+    }
+    for (int i = 0; i <= np; ++i) {
+        b[i] = exp(-(sigma[i] / kappa[i] + alpha[i]) * dt / kEps0);
+        if ((sigma[i] == 0.0) && (alpha[i] == 0.0)) c[i] = 0.0;
+        else c[i] = sigma[i] * (b[i] - 1.0) / (sigma[i] + kappa[i] * alpha[i]) / kappa[i] / del;
+    }
+}
+
+// H-side grading, CPML.cpp:185-229, every entry including np-1
+void grade_h(std::vector<double> &kappa, std::vector<double> &b, std::vector<double> &c, bool first, int np,
+             double dt, double del, double m, double ma, double sigmax, double kapmax, double alpmax)
+{
+    std::vector<double> sigma(np), alpha(np);
+    kappa.assign(np, 0); b.assign(np + 1, 0); c.assign(np + 1, 0);
+    for (int i = 1; i <= np; ++i) {
+        double ps, pa;
+        if (first) { ps = pow(((np - i + 0.5) / np), m); pa = pow(((i - 0.5) / np), ma); }
+        else { ps = pow(((i - 0.5) / np), m); pa = pow(((np - i + 0.5) / np), ma); }
+        sigma[i - 1] = sigmax * ps;
+        kappa[i - 1] = 1.0 + (kapmax - 1.0) * ps;
+        alpha[i - 1] = alpmax * pa;
+    }
+    for (int i = 0; i < np; ++i) {
+        b[i] = exp(-(sigma[i] / kappa[i] + alpha[i]) * dt / kEps0);
+        if ((sigma[i] == 0.0) && (alpha[i] == 0.0)) c[i] = 0.0;
+        else c[i] = sigma[i] * (b[i] - 1.0) / (sigma[i] + kappa[i] * alpha[i]) / kappa[i] / del;
+    }
+}
+
+// sorted cell list (device linear index) of cells with a given ID inside the
+// E-update range, plus per (k, j, 32-wide x segment) start offsets
+cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cell, int32_t **d_seg)
+{
+    const Dims &d = g->d;
+    std::vector<int64_t> cells;
+    const int nseg = d.px / 32;
+    std::vector<int32_t> seg((size_t)(d.nz + 1) * (d.ny + 1) * nseg, 0);
+    for (int k = 0; k <= d.nz; ++k)
+        for (int j = 0; j <= d.ny; ++j)
+            for (int s = 0; s < nseg; ++s) {
+                seg[((size_t)k * (d.ny + 1) + j) * nseg + s] = (int32_t)cells.size();
+                if (k < 1 || k >= d.nz || j < 1 || j >= d.ny) continue;
+                for (int i = s * 32; i < s * 32 + 32 && i < d.nx; ++i) {
+                    if (i < 1) continue;
+                    const int64_t q = d.idx(i, j, k);
+                    if (g->ids_dev[q] == id_match) cells.push_back(q);
+                }
+            }
+    REQUIRE(cells.size() < (size_t)INT32_MAX, CPS_E_INVALID, "too many cells in one compacted list");
+    *count = (int64_t)cells.size();
+    cps_status s = dalloc(g, (void **)d_cell, cells.size() * sizeof(int64_t));
+    if (s) return s;
+    s = dalloc(g, (void **)d_seg, seg.size() * sizeof(int32_t));
+    if (s) return s;
+    if (!cells.empty()) { s = upload_raw(g, *d_cell, cells.data(), cells.size() * sizeof(int64_t)); if (s) return s; }
+    return upload_raw(g, *d_seg, seg.data(), seg.size() * sizeof(int32_t));
+}
+
+void gain_initial_state(cps_grid *g, std::vector<double> &words, int64_t n)
+{
+    // SoA [word][cell]; FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197); FP32 keeps offsets (all 0)
+    const int nw = g->fp32 ? kG32Words : kG64Words;
+    words.assign((size_t)nw * n, 0.0);
+    if (!g->fp32)
+        for (int64_t c = 0; c < n; ++c) {
+            words[(size_t)21 * n + c] = 1.0;
+            words[(size_t)22 * n + c] = 1.0;
+        }
+}
+
+cps_status flush_dft(cps_grid *g, PortState &P);
+
+cps_status ensure_sources(cps_grid *g)
+{
+    if (!g->src_dirty) return CPS_OK;
+    for (void *p : {(void *)g->d_src_idx, (void *)g->d_src_comp, (void *)g->d_src_off, (void *)g->d_src_len,
+                    (void *)g->d_src_wave})
+        dfree(g, p);
+    const size_t ns = g->src.size();
+    std::vector<int64_t> idx(ns);
+    std::vector<int32_t> comp(ns), off(ns), len(ns);
+    std::vector<double> wave;
+    for (size_t s = 0; s < ns; ++s) {
+        idx[s] = g->src[s].idx; comp[s] = g->src[s].comp;
+        off[s] = (int32_t)wave.size(); len[s] = (int32_t)g->src[s].wave.size();
+        wave.insert(wave.end(), g->src[s].wave.begin(), g->src[s].wave.end());
+    }
+    cps_status s;
+    if ((s = dalloc(g, (void **)&g->d_src_idx, ns * 8)) || (s = dalloc(g, (void **)&g->d_src_comp, ns * 4)) ||
+        (s = dalloc(g, (void **)&g->d_src_off, ns * 4)) || (s = dalloc(g, (void **)&g->d_src_len, ns * 4)) ||
+        (s = dalloc(g, (void **)&g->d_src_wave, wave.size() * 8)))
+        return s;
+    if ((s = upload_raw(g, g->d_src_idx, idx.data(), ns * 8)) || (s = upload_raw(g, g->d_src_comp, comp.data(), ns * 4)) ||
+        (s = upload_raw(g, g->d_src_off, off.data(), ns * 4)) || (s = upload_raw(g, g->d_src_len, len.data(), ns * 4)) ||
+        (s = upload_raw(g, g->d_src_wave, wave.data(), wave.size() * 8)))
+        return s;
+    g->src_dirty = false;
+    return CPS_OK;
+}
+
+// ---------------------------------------------------------- step pieces
+
+template <typename T>
+void op_inject(cps_grid *g, int isH, double n, uint32_t mask)
+{
+    if (!g->tfsf_on || g->ntg[isH] == 0) return;
+    const FieldView<T> f = field_view<T>(g);
+    launch_inject<T>(f, g->d_tg[isH], g->ntg[isH], g->d_ct[isH], (const T *)(isH ? g->d_einc : g->d_hinc),
+                     g->tp.Nt, n, mask, g->stream);
+    g->launches++;
+}
+
+template <typename T>
+void op_sources(cps_grid *g, int n)
+{
+    if (g->src.empty()) return;
+    launch_sources<T>(field_view<T>(g), (int)g->src.size(), g->d_src_idx, g->d_src_comp, g->d_src_wave,
+                      g->d_src_off, g->d_src_len, n, g->stream);
+    g->launches++;
+}
+
+template <typename T>
+cps_status op_port(cps_grid *g, PortState &P, int64_t n)
+{
+    if (P.fill == P.slots) {
+        cps_status s = flush_dft(g, P);
+        if (s) return s;
+    }
+    if (P.fill == 0) P.ring_n0 = n;
+    T *slot = (T *)P.d_ring + (int64_t)P.fill * 6 * P.npts;
+    launch_port_gather<T>(field_view<T>(g), P.d_idx, P.npts, slot, g->stream);
+    g->launches++;
+    P.last_slot = P.fill;
+    P.fill++;
+    if (P.nfreq == 0) P.fill = 0;  // no DFT: the ring holds the last sample only
+    return CPS_OK;
+}
+
+template <typename T>
+cps_status flush_dft_T(cps_grid *g, PortState &P)
+{
+    if (P.nfreq == 0 || P.fill == 0) return CPS_OK;
+    const size_t need = (size_t)P.slots * P.nfreq * 2 * sizeof(double);
+    if (g->phasor_cap < need) {
+        dfree(g, g->d_phasor);
+        cps_status s = dalloc(g, (void **)&g->d_phasor, need);
+        if (s) return s;
+        g->phasor_cap = need;
+    }
+    launch_port_dft<T>((const T *)P.d_ring, P.npts, P.fill, P.ring_n0, g->desc.dt, P.d_omega, P.nfreq, P.d_comps,
+                       P.ncomp, P.d_acc, g->d_phasor, g->stream);
+    g->launches += 2;
+    // keep the last sample readable: move it to slot 0
+    if (P.last_slot > 0) {
+        CK(cudaMemcpyAsync(P.d_ring, (T *)P.d_ring + (int64_t)P.last_slot * 6 * P.npts, sizeof(T) * 6 * P.npts,
+                           cudaMemcpyDeviceToDevice, g->stream));
+        P.last_slot = 0;
+    }
+    P.fill = 0;
+    return CPS_OK;
+}
+
+cps_status flush_dft(cps_grid *g, PortState &P)
+{
+    return g->fp32 ? flush_dft_T<float>(g, P) : flush_dft_T<double>(g, P);
+}
+
+template <typename T>
+cps_status step_T(cps_grid *g, int nsteps, int path)
+{
+    cps_status s = ensure_sources(g);
+    if (s) return s;
+    const FieldView<T> f = field_view<T>(g);
+    const PmlView<T> p = pml_view<T>(g);
+    const DlView<T> D = dl_view<T>(g);
+    const GainView<T> G = gain_view<T>(g);
+    for (int it = 0; it < nsteps; ++it) {
+        const int64_t n = g->step;
+        if (path == CPS_PATH_PLAIN) {
+            launch_h_bulk<T>(f, g->stream);
+            op_inject<T>(g, 1, (double)n, CPS_FACE_ALL);
+            if (g->pml_on) launch_h_pml<T>(f, p, g->stream);
+            launch_e_bulk<T>(f, g->stream);
+            if (g->dl_on) launch_dl<T>(f, D, g->stream);
+            if (g->gain_on) {
+                launch_gain<T>(f, G, 0, g->stream);
+                launch_gain<T>(f, G, 1, g->stream);
+                launch_gain<T>(f, G, 2, g->stream);
+            }
+            op_inject<T>(g, 0, (double)n, CPS_FACE_ALL);
+            op_sources<T>(g, (int)n);
+            if (g->pml_on) launch_e_pml<T>(f, p, g->stream);
+            g->launches += 2 + (g->pml_on ? 12 : 0) + (g->dl_on ? 1 : 0) + (g->gain_on ? 3 : 0);
+        } else {
+            const bool timed = g->timing_stride > 0 && n % g->timing_stride == 0 &&
+                               g->ev_used + 4 <= (int)g->ev.size();
+            if (timed) cudaEventRecord(g->ev[g->ev_used], g->stream);
+            launch_h_fused<T>(f, p, g->shape, g->stream);
+            if (timed) cudaEventRecord(g->ev[g->ev_used + 1], g->stream);
+            op_inject<T>(g, 1, (double)n, CPS_FACE_ALL);
+            if (timed) cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
+            launch_e_fused<T>(f, p, D, G, g->shape, g->stream);
+            if (timed) {
+                cudaEventRecord(g->ev[g->ev_used + 3], g->stream);
+                g->ev_used += 4;
+            }
+            op_inject<T>(g, 0, (double)n, CPS_FACE_ALL);
+            op_sources<T>(g, (int)n);
+            g->launches += 2;
+        }
+        for (PortState &P : g->ports) {
+            s = op_port<T>(g, P, n);
+            if (s) return s;
+        }
+        g->step++;
+    }
+    cudaError_t e = cudaGetLastError();
+    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+    return CPS_OK;
+}
+
+cps_status need_setup(const cps_grid *g)
+{
+    REQUIRE(g, CPS_E_INVALID, "grid handle is NULL");
+    REQUIRE(g->nmedia > 0, CPS_E_STATE, "media are not set (cps_grid_set_media)");
+    REQUIRE(g->ids_set, CPS_E_STATE, "material IDs are not uploaded (cps_grid_upload_ids)");
+    return CPS_OK;
+}
+
+}  // namespace
+
+// ================================================================ lifetime
+
+extern "C" cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out)
+{
+    REQUIRE(desc && out, CPS_E_INVALID, "cps_grid_create: NULL argument");
+    *out = nullptr;
+    REQUIRE(desc->nx >= 4 && desc->ny >= 4 && desc->nz >= 4, CPS_E_INVALID, "grid needs at least 4 cells per axis");
+    REQUIRE(desc->nx < 16384 && desc->ny < 16384 && desc->nz < 16384, CPS_E_INVALID, "grid edge too large");
+    REQUIRE(desc->dx > 0 && desc->dy > 0 && desc->dz > 0, CPS_E_INVALID, "cell sizes must be positive");
+    REQUIRE(desc->precision == CPS_FP64 || desc->precision == CPS_FP32, CPS_E_INVALID, "precision must be CPS_FP64 or CPS_FP32");
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    REQUIRE(desc->device >= 0 && desc->device < ndev, CPS_E_INVALID, "no such CUDA device");
+    CK(cudaSetDevice(desc->device));
+    cps_grid *g = new cps_grid();
+    g->desc = *desc;
+    if (!(g->desc.dt > 0)) g->desc.dt = cps_courant_dt(desc->dx, desc->dy, desc->dz);
+    g->fp32 = desc->precision == CPS_FP32;
+    g->esz = g->fp32 ? 4 : 8;
+    g->d.nx = desc->nx; g->d.ny = desc->ny; g->d.nz = desc->nz;
+    g->d.px = (desc->nx + 1 + kXPad - 1) / kXPad * kXPad;
+    g->d.pxy = (int64_t)g->d.px * (desc->ny + 1);
+    g->elems = g->d.pxy * (desc->nz + 1);
+    cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete g; return CPS_E_CUDA; }
+    g->own_stream = true;
+    cps_status s = CPS_OK;
+    for (int c = 0; c < 6 && !s; ++c) s = dalloc(g, &g->F[c], (size_t)g->elems * g->esz);
+    if (!s) s = dalloc(g, (void **)&g->d_id, (size_t)g->elems);
+    if (!s) s = dalloc(g, &g->d_media, 4 * 256 * g->esz);
+    if (!s) s = dalloc(g, (void **)&g->d_counter, sizeof(unsigned long long));
+    if (s) { cps_grid_destroy(g); return s; }
+    g->ids_dev.assign((size_t)g->elems, 0);
+    // stretched coordinates start at 1/delta (Structure.cpp:425-445)
+    for (int w = 0; w < 12; ++w) {
+        const int axis = (w % 6) < 2 ? 2 : ((w % 6) < 4 ? 1 : 0);
+        const double del = axis == 0 ? desc->dx : axis == 1 ? desc->dy : desc->dz;
+        g->st[w].assign(kStretchLen(g, w), 1.0 / del);
+    }
+    s = push_stretch(g);
+    if (s) { cps_grid_destroy(g); return s; }
+    e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); cps_grid_destroy(g); return CPS_E_CUDA; }
+    *out = g;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_destroy(cps_grid *g)
+{
+    if (!g) return CPS_OK;
+    cudaSetDevice(g->desc.device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    for (auto &a : g->owned) cudaFree(a.first);
+    g->owned.clear();
+    for (auto &e : g->ev) cudaEventDestroy(e);
+    if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
+    delete g;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_info(const cps_grid *g, cps_grid_desc *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "NULL argument");
+    *out = g->desc;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_bytes(const cps_grid *g, int64_t *bytes)
+{
+    REQUIRE(g && bytes, CPS_E_INVALID, "NULL argument");
+    size_t total = 0;
+    for (const auto &a : g->owned) total += a.second;
+    *bytes = (int64_t)total;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_set_stream(cps_grid *g, void *stream)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    CK(cudaStreamSynchronize(g->stream));
+    if (g->own_stream && stream) { cudaStreamDestroy(g->stream); g->own_stream = false; }
+    if (stream) g->stream = (cudaStream_t)stream;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_get_stream(const cps_grid *g, void **stream)
+{
+    REQUIRE(g && stream, CPS_E_INVALID, "NULL argument");
+    *stream = (void *)g->stream;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_synchronize(cps_grid *g)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+// ================================================================ geometry
+
+extern "C" cps_status cps_grid_set_media(cps_grid *g, int32_t n, const double *epsR, const double *muR,
+                                         const double *sig, const double *sigM)
+{
+    REQUIRE(g && epsR && muR && sig && sigM, CPS_E_INVALID, "cps_grid_set_media: NULL argument");
+    REQUIRE(n >= 1 && n <= 256, CPS_E_INVALID, "cps_grid_set_media: 1..256 media");
+    const double dt = g->desc.dt;
+    for (int i = 0; i < n; ++i) {
+        REQUIRE(epsR[i] > 0 && muR[i] > 0, CPS_E_INVALID, "cps_grid_set_media: epsR and muR must be positive");
+        // Structure.cpp:446-451
+        g->aE[i] = (2.0 * kEps0 * epsR[i] - sig[i] * dt) / (2.0 * kEps0 * epsR[i] + sig[i] * dt);
+        g->bE[i] = (2.0 * dt) / (2.0 * kEps0 * epsR[i] + sig[i] * dt);
+        g->aH[i] = (2.0 * kMu0 * muR[i] - sigM[i] * dt) / (2.0 * kMu0 * muR[i] + sigM[i] * dt);
+        g->bH[i] = (2.0 * dt) / (2.0 * kMu0 * muR[i] + sigM[i] * dt);
+    }
+    g->nmedia = n;
+    std::vector<double> t(1024, 0.0);
+    for (int i = 0; i < 256; ++i) { t[i] = g->aE[i]; t[256 + i] = g->bE[i]; t[512 + i] = g->aH[i]; t[768 + i] = g->bH[i]; }
+    return upload_real(g, g->d_media, t.data(), t.size());
+}
+
+extern "C" cps_status cps_grid_upload_ids(cps_grid *g, const uint8_t *ids)
+{
+    REQUIRE(g && ids, CPS_E_INVALID, "cps_grid_upload_ids: NULL argument");
+    REQUIRE(!g->dl_on && !g->gain_on && !g->pml_on, CPS_E_STATE,
+            "cps_grid_upload_ids: IDs must be set before the physics modules are initialised");
+    const Dims &d = g->d;
+    std::fill(g->ids_dev.begin(), g->ids_dev.end(), 0);
+    int maxid = 0;
+    size_t q = 0;
+    for (int i = 0; i <= d.nx; ++i)
+        for (int j = 0; j <= d.ny; ++j)
+            for (int k = 0; k <= d.nz; ++k) {
+                const uint8_t v = ids[q++];
+                maxid = std::max<int>(maxid, v);
+                g->ids_dev[d.idx(i, j, k)] = v;
+            }
+    REQUIRE(g->nmedia == 0 || maxid < g->nmedia, CPS_E_INVALID,
+            "cps_grid_upload_ids: an ID has no medium (set the media first or extend them)");
+    cps_status s = upload_raw(g, g->d_id, g->ids_dev.data(), g->ids_dev.size());
+    if (s) return s;
+    g->ids_set = true;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_download_ids(const cps_grid *g, uint8_t *ids)
+{
+    REQUIRE(g && ids, CPS_E_INVALID, "NULL argument");
+    const Dims &d = g->d;
+    size_t q = 0;
+    for (int i = 0; i <= d.nx; ++i)
+        for (int j = 0; j <= d.ny; ++j)
+            for (int k = 0; k <= d.nz; ++k) ids[q++] = g->ids_dev[d.idx(i, j, k)];
+    return CPS_OK;
+}
+
+// ================================================================ modules
+
+extern "C" cps_status cps_pml_init(cps_grid *g, const cps_pml_params *pp)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    REQUIRE(pp, CPS_E_INVALID, "cps_pml_init: NULL params");
+    REQUIRE(!g->pml_on, CPS_E_STATE, "cps_pml_init: CPML already initialised");
+    const int nax[3] = {g->d.nx, g->d.ny, g->d.nz};
+    for (int a = 0; a < 3; ++a) {
+        const int n1 = pp->npml[2 * a], n2 = pp->npml[2 * a + 1];
+        REQUIRE(n1 == n2, CPS_E_INVALID,
+                "cps_pml_init: both ends of an axis need the same thickness (the reference folds the second-end "
+                "kappa with the first-end count, CPML.cpp:374)");
+        REQUIRE(n1 >= 1 && 2 * n1 < nax[a] - 1, CPS_E_INVALID, "cps_pml_init: thickness must be >= 1 and leave an interior");
+    }
+    REQUIRE(pp->m >= 0 && pp->kapmax >= 1.0 && pp->alpmax >= 0, CPS_E_INVALID, "cps_pml_init: bad grading parameters");
+    g->pml = *pp;
+    const double eta0 = sqrt(kMu0 / kEps0);
+    const double del[3] = {g->desc.dx, g->desc.dy, g->desc.dz};
+    // stretch arrays: E side (cEzy,cEyz | cEzx,cExz | cExy,cEyx), H side likewise
+    const int wE[3][2] = {{4, 5}, {2, 3}, {0, 1}};
+    const int wH[3][2] = {{10, 11}, {8, 9}, {6, 7}};
+    for (int a = 0; a < 3; ++a) {
+        const double sigmax = pp->sig_ratio * (0.8 * (pp->m + 1) / (del[a] * eta0));
+        for (int end = 0; end < 2; ++end) {
+            const int f = 2 * a + end, np = pp->npml[f];
+            std::vector<double> kap, kapH, bh, ch;
+            grade_e(kap, g->pbE[f], g->pcE[f], end == 0, np, g->desc.dt, del[a], pp->m, pp->malp, sigmax, pp->kapmax, pp->alpmax);
+            grade_h(kapH, g->pbH[f], g->pcH[f], end == 0, np, g->desc.dt, del[a], pp->m, pp->malp, sigmax, pp->kapmax, pp->alpmax);
+            // kappa folding, CPML.cpp:361-365, 374-378, 446-450, 459-463
+            for (int q = 0; q < 2; ++q) {
+                std::vector<double> &se = g->st[wE[a][q]], &sh = g->st[wH[a][q]];
+                if (end == 0) {
+                    for (int i = 0; i <= np; ++i) se[i] = se[i] / kap[i];
+                    for (int i = 0; i < np; ++i) sh[i] = sh[i] / kapH[i];
+                } else {
+                    const int base = nax[a] - np;
+                    for (int i = 0; i < np; ++i) se[base + i] = se[base + i] / kap[i];
+                    for (int i = 0; i < np; ++i) sh[base + i] = sh[base + i] / kapH[i];
+                }
+            }
+        }
+    }
+    g->cpmlE = g->desc.dt / kEps0;  // CPML.cpp:524
+    g->cpmlH = g->bH[0];            // CPML.cpp:525
+    // coefficient tables: per face bE cE bH cH, each np+1
+    std::vector<double> coef;
+    for (int f = 0; f < 6; ++f) {
+        const int np = pp->npml[f];
+        for (std::vector<double> *v : {&g->pbE[f], &g->pcE[f], &g->pbH[f], &g->pcH[f]}) {
+            std::vector<double> t = *v;
+            t.resize(np + 1, 0.0);
+            coef.insert(coef.end(), t.begin(), t.end());
+        }
+    }
+    if ((s = dalloc(g, &g->d_pcoef, coef.size() * g->esz))) return s;
+    if ((s = upload_real(g, g->d_pcoef, coef.data(), coef.size()))) return s;
+    const Dims &d = g->d;
+    for (int f = 0; f < 6; ++f) {
+        const int np = pp->npml[f];
+        size_t n;
+        if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * (np + 1);
+        else if (f < 4) n = (size_t)(d.nz + 1) * (np + 1) * d.px;
+        else n = (size_t)(np + 1) * (d.ny + 1) * d.px;
+        for (int q = 0; q < 4; ++q)
+            if ((s = dalloc(g, &g->d_q[f][q], n * g->esz))) return s;
+    }
+    if ((s = push_stretch(g))) return s;
+    g->pml_on = true;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    REQUIRE(p, CPS_E_INVALID, "cps_dl_init: NULL params");
+    REQUIRE(!g->dl_on, CPS_E_STATE, "cps_dl_init: already initialised");
+    REQUIRE(p->nD >= 0 && p->nL >= 0 && p->nD <= kMaxPoles && p->nL <= kMaxPoles && p->nD + p->nL > 0,
+            CPS_E_INVALID, "cps_dl_init: 0..8 Drude and 0..8 Lorentz poles, at least one");
+    REQUIRE(p->epsInf > 0, CPS_E_INVALID, "cps_dl_init: epsInf must be positive");
+    const double dt = g->desc.dt;
+    DlCoef<double> &D = g->dlc;
+    memset(&D, 0, sizeof(D));
+    D.nD = p->nD; D.nL = p->nL; D.stride = p->nD + 2 * p->nL + 1; D.dt = dt; D.inv2dt = 1.0 / (2.0 * dt);
+    // Drude_Lorentz.cpp:65-108
+    double temp1 = 0, temp2 = 0;
+    for (int q = 0; q < p->nD; ++q) {
+        const double omega = p->fD[q] * 2.0 * kPi, gamma = p->gD[q] * 2.0 * kPi;
+        D.kappa[q] = (1.0 - gamma * dt / 2.0) / (1.0 + gamma * dt / 2.0);
+        D.beta[q] = (omega * omega * kEps0 * dt / 2.0) / (1.0 + gamma * dt / 2.0);
+        temp1 = temp1 + D.beta[q];
+    }
+    for (int q = 0; q < p->nL; ++q) {
+        const double omega = p->fL[q] * 2.0 * kPi, delta = p->dL[q] * 2.0 * kPi;
+        D.alpha[q] = (2.0 - omega * omega * dt * dt) / (1.0 + delta * dt);
+        D.xi[q] = (delta * dt - 1.0) / (1.0 + delta * dt);
+        D.gammaL[q] = (kEps0 * p->depsL[q] * omega * omega * dt * dt) / (1.0 + delta * dt);
+        temp2 = temp2 + D.gammaL[q];
+    }
+    const double den = 2.0 * kEps0 * p->epsInf + p->sigma * dt + dt * temp1 + temp2 / 2.0;
+    // literal: C1 and C5 as Drude_Lorentz.cpp:96,106; else the values of the
+    // ADE discretisation (E^n coefficient with -sigma dt - dt sum(beta), J_L
+    // coefficient with the factor dt)
+    if (p->literal) D.C1 = (2.0 * kEps0 * p->epsInf + p->sigma * dt + dt * temp1) / den;
+    else D.C1 = (2.0 * kEps0 * p->epsInf - p->sigma * dt - dt * temp1) / den;
+    D.C2 = temp2 / 2.0 / den;
+    D.C3 = 2.0 * dt / den;
+    for (int q = 0; q < p->nD; ++q) D.C4[q] = (1.0 + D.kappa[q]) * dt / den;
+    for (int q = 0; q < p->nL; ++q) {
+        D.C5[q] = p->literal ? (1.0 + D.alpha[q]) / den : (1.0 + D.alpha[q]) * dt / den;
+        D.C6[q] = D.xi[q] * dt / den;
+    }
+    if ((s = build_list(g, CPS_ID_DISPERSIVE, &g->dl_n, &g->d_dl_cell, &g->d_dl_seg))) return s;
+    if ((s = dalloc(g, &g->d_dl_state, (size_t)g->dl_n * 3 * D.stride * g->esz))) return s;
+    g->dl_on = true;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    REQUIRE(p, CPS_E_INVALID, "cps_gain_init: NULL params");
+    REQUIRE(!g->gain_on, CPS_E_STATE, "cps_gain_init: already initialised");
+    REQUIRE(p->gain_id >= 0 && p->gain_id < 256 && p->gain_id != CPS_ID_DISPERSIVE && p->gain_id != CPS_ID_PEC,
+            CPS_E_INVALID, "cps_gain_init: gain_id must be a plain medium (not 2 or 4)");
+    REQUIRE(p->lambda_a > 0 && p->lambda_b > 0 && p->t30 > 0 && p->t32 > 0 && p->t21 > 0 && p->t10 > 0 && p->N_0 > 0,
+            CPS_E_INVALID, "cps_gain_init: wavelengths, lifetimes and N_0 must be positive");
+    const double dt = g->desc.dt, dx = g->desc.dx, dy = g->desc.dy;
+    GainCoef &G = g->gc;
+    // FourLevelLaser.cpp:96-105, 202-209
+    const double omega_a = 2.0 * kPi * kC / p->lambda_a, omega_b = 2.0 * kPi * kC / p->lambda_b;
+    const double zeta_a = 6.0 * kPi * kEps0 * kC * kC * kC / (omega_a * omega_a * p->t21);
+    const double zeta_b = 6.0 * kPi * kEps0 * kC * kC * kC / (omega_b * omega_b * p->t30);
+    G.CPa1 = (2.0 - omega_a * omega_a * dt * dt) / (1.0 + p->gamma_a * dt / 2.0);
+    G.CPa2 = (p->gamma_a * dt / 2.0 - 1.0) / (1.0 + p->gamma_a * dt / 2.0);
+    G.CPa3 = dt * dt * zeta_a / (1.0 + p->gamma_a * dt / 2.0);
+    G.CPb1 = (2.0 - omega_b * omega_b * dt * dt) / (1.0 + p->gamma_b * dt / 2.0);
+    G.CPb2 = (p->gamma_b * dt / 2.0 - 1.0) / (1.0 + p->gamma_b * dt / 2.0);
+    G.CPb3 = dt * dt * zeta_b / (1.0 + p->gamma_b * dt / 2.0);
+    G.CEP = 2.0 * p->N_0 * dx * dy * dx / kEps0 / dt;
+    G.t30 = p->t30; G.t32 = p->t32; G.t21 = p->t21; G.t10 = p->t10;
+    G.t30t32dt = p->t30 * p->t32 * dt; G.t30t32_2 = 2.0 * p->t30 * p->t32; G.t30dt = p->t30 * dt;
+    G.t32dt = p->t32 * dt; G.dt_2 = 2.0 / dt; G.homega_bdt = kHPlanck * omega_b * dt / 2.0 / kPi;
+    G.t10t21dt = p->t10 * p->t21 * dt; G.t10t21_2 = 2.0 * p->t10 * p->t21; G.t10dt = p->t10 * dt;
+    G.t21dt = p->t21 * dt; G.t21_2 = p->t21 / 2.0; G.homega_adt = kHPlanck * omega_a * dt / 2.0 / kPi;
+    G.t32t21dt = p->t32 * p->t21 * dt; G.t32t21_2 = 2.0 * p->t32 * p->t21; G.t32_2 = p->t32 / 2.0;
+    G.pump_dt = p->pump_rate * dt;
+    G.scaleP = g->fp32 ? G.CEP : 1.0;
+    g->gain_id = p->gain_id;
+    if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg))) return s;
+    const int nw = g->fp32 ? kG32Words : kG64Words;
+    if ((s = dalloc(g, &g->d_g_state, (size_t)g->g_n * nw * g->esz))) return s;
+    std::vector<double> init;
+    gain_initial_state(g, init, g->g_n);
+    if ((s = upload_real(g, g->d_g_state, init.data(), init.size()))) return s;
+    g->gain_on = true;
+    return CPS_OK;
+}
+
+namespace {
+
+// Gaussian-beam profile and delay of one boundary point (TF_SF.cpp:156-166, repeated per face)
+void tfsf_point(double x, double y, double z, double kx, double ky, double kz, double kabs, double w0, double z0,
+                double zR, double l0, double dt, double *delay, double *profile)
+{
+    const double r2 = x * x + y * y + z * z;
+    double r_dot_k = (x * kx + y * ky + z * kz) / kabs;
+    const double rho2 = r2 - r_dot_k * r_dot_k;
+    r_dot_k = r_dot_k - z0;
+    const double wz = w0 * sqrt(1 + r_dot_k * r_dot_k / (zR * zR));
+    *profile = exp(-rho2 / wz / wz);
+    *delay = ((x * kx + y * ky + z * kz) / kC - l0) / dt;
+}
+
+}  // namespace
+
+extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    REQUIRE(p, CPS_E_INVALID, "cps_tfsf_init: NULL params");
+    REQUIRE(!g->tfsf_on, CPS_E_STATE, "cps_tfsf_init: already initialised");
+    const Dims &d = g->d;
+    const double dx = g->desc.dx, dy = g->desc.dy, dz = g->desc.dz, dt = g->desc.dt;
+    const int i1 = p->n[0], i2 = d.nx - p->n[1], j1 = p->n[2], j2 = d.ny - p->n[3], k1 = p->n[4], k2 = d.nz - p->n[5];
+    REQUIRE(i1 >= 1 && j1 >= 1 && k1 >= 1 && i2 + 1 <= d.nx - 1 && j2 + 1 <= d.ny - 1 && k2 + 1 <= d.nz - 1 &&
+                i2 > i1 && j2 > j1 && k2 > k1,
+            CPS_E_INVALID, "cps_tfsf_init: TF/SF box must lie inside the grid with one cell to spare");
+    REQUIRE(p->Nt >= 1 && p->lambda > 0 && p->w0 > 0, CPS_E_INVALID, "cps_tfsf_init: bad Nt, lambda or w0");
+    g->tp = *p;
+    const double theta = p->theta_deg * kPi / 180.0, phi = p->phi_deg * kPi / 180.0, psi = p->psi_deg * kPi / 180.0;
+    const double E0 = p->E0, eta0 = sqrt(kMu0 / kEps0);
+    // Taflove polarisation and direction, TF_SF.cpp:112-122
+    const double E0x = E0 * (cos(psi) * sin(phi) - sin(psi) * cos(theta) * cos(phi));
+    const double E0y = E0 * (-cos(psi) * cos(phi) - sin(psi) * cos(theta) * sin(phi));
+    const double E0z = E0 * sin(psi) * sin(theta);
+    const double H0x = E0 / eta0 * (sin(psi) * sin(phi) + cos(psi) * cos(theta) * cos(phi));
+    const double H0y = E0 / eta0 * (-sin(psi) * cos(phi) + cos(psi) * cos(theta) * sin(phi));
+    const double H0z = -E0 / eta0 * cos(psi) * sin(theta);
+    const double kx = sin(theta) * cos(phi), ky = sin(theta) * sin(phi), kz = cos(theta);
+    const double kabs = sqrt(kx * kx + ky * ky + kz * kz);
+    const int ci[2] = {i1, i2}, cj[2] = {j1, j2}, ck[2] = {k1, k2};
+    double l0 = 0;  // earliest corner, TF_SF.cpp:124-138
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) {
+                const double v = (kx * (ci[a] - p->i0) * dx + ky * (cj[b] - p->j0) * dy + kz * (ck[c] - p->k0) * dz) / kC;
+                if ((a | b | c) == 0 || l0 > v) l0 = v;
+            }
+    const double zR = kPi * p->w0 * p->w0 / p->lambda;
+    const double CE[3] = {dt / (kEps0 * dx), dt / (kEps0 * dy), dt / (kEps0 * dz)};
+    const double CH[3] = {dt / (kMu0 * dx), dt / (kMu0 * dy), dt / (kMu0 * dz)};
+    // signed coefficients per face and correction (TF_SF.cpp:988-1089, 1201-1300)
+    double cE[6][2], cH[6][2];
+    cE[kFX1][0] = CE[0] * H0z; cE[kFX1][1] = -(CE[0] * H0y);
+    cE[kFX2][0] = -(CE[0] * H0z); cE[kFX2][1] = CE[0] * H0y;
+    cE[kFY1][0] = -(CE[1] * H0z); cE[kFY1][1] = CE[1] * H0x;
+    cE[kFY2][0] = CE[1] * H0z; cE[kFY2][1] = -(CE[1] * H0x);
+    cE[kFZ1][0] = CE[2] * H0y; cE[kFZ1][1] = -(CE[2] * H0x);
+    cE[kFZ2][0] = -(CE[2] * H0y); cE[kFZ2][1] = CE[2] * H0x;
+    cH[kFX1][0] = CH[0] * E0y; cH[kFX1][1] = -(CH[0] * E0z);
+    cH[kFX2][0] = -(CH[0] * E0y); cH[kFX2][1] = CH[0] * E0z;
+    cH[kFY1][0] = -(CH[1] * E0x); cH[kFY1][1] = CH[1] * E0z;
+    cH[kFY2][0] = CH[1] * E0x; cH[kFY2][1] = -(CH[1] * E0z);
+    cH[kFZ1][0] = CH[2] * E0x; cH[kFZ1][1] = -(CH[2] * E0y);
+    cH[kFZ2][0] = -(CH[2] * E0x); cH[kFZ2][1] = CH[2] * E0y;
+    // components of correction 1/2: x faces (Ey|Hz, Ez|Hy), y faces (Ex|Hz, Ez|Hx), z faces (Ex|Hy, Ey|Hx)
+    const int compE[3][2] = {{CPS_EY, CPS_EZ}, {CPS_EX, CPS_EZ}, {CPS_EX, CPS_EY}};
+    const int compH[3][2] = {{CPS_HZ, CPS_HY}, {CPS_HZ, CPS_HX}, {CPS_HY, CPS_HX}};
+    const int order[6] = {kFY1, kFY2, kFX1, kFX2, kFZ1, kFZ2};
+    for (int isH = 0; isH < 2; ++isH) {
+        std::map<int64_t, std::vector<InjContrib>> per;  // key = idx * 8 + comp
+        std::vector<int64_t> keys;                      // first-seen order
+        for (int oi = 0; oi < 6; ++oi) {
+            const int f = order[oi], ax = f / 2, far = f & 1;
+            int u1, u2, v1, v2;
+            if (ax == 0) { u1 = j1; u2 = j2; v1 = k1; v2 = k2; }
+            else if (ax == 1) { u1 = i1; u2 = i2; v1 = k1; v2 = k2; }
+            else { u1 = i1; u2 = i2; v1 = j1; v2 = j2; }
+            for (int which = 0; which < 2; ++which) {
+                // E1 covers [u1,u2) x [v1,v2], E2 [u1,u2] x [v1,v2); the x-face H
+                // strips add nothing in the reference (TF_SF.cpp:1244-1251,
+                // 1260-1267 read unset point members), so x-face H covers [u1,u2) x [v1,v2)
+                int ue = which == 0 ? u2 - 1 : u2, ve = which == 0 ? v2 : v2 - 1;
+                if (isH && ax == 0) { ue = u2 - 1; ve = v2 - 1; }
+                const int comp = isH ? compH[ax][which] : compE[ax][which];
+                const double coef = isH ? cH[f][which] : cE[f][which];
+                for (int u = u1; u <= ue; ++u)
+                    for (int v = v1; v <= ve; ++v) {
+                        int i, j, k;
+                        double x, y, z;
+                        if (ax == 0) {
+                            i = far ? i2 : i1; j = u; k = v;
+                            x = isH ? dx * (i - p->i0) : dx * (far ? (i - p->i0 + 0.5) : (i - p->i0 - 0.5));
+                            y = dy * (j - p->j0); z = dz * (k - p->k0);
+                            if (isH) i += far ? 1 : -1;
+                        } else if (ax == 1) {
+                            i = u; j = far ? j2 : j1; k = v;
+                            x = dx * (i - p->i0);
+                            y = isH ? dy * (j - p->j0) : dy * (far ? (j - p->j0 + 0.5) : (j - p->j0 - 0.5));
+                            z = dz * (k - p->k0);
+                            if (isH) j += far ? 1 : -1;
+                        } else {
+                            i = u; j = v; k = far ? k2 : k1;
+                            x = dx * (i - p->i0); y = dy * (j - p->j0);
+                            z = isH ? dz * (k - p->k0) : dz * (far ? (k - p->k0 + 0.5) : (k - p->k0 - 0.5));
+                            if (isH) k += far ? 1 : -1;
+                        }
+                        InjContrib c;
+                        tfsf_point(x, y, z, kx, ky, kz, kabs, p->w0, p->z0, zR, l0, dt, &c.delay, &c.profile);
+                        c.coef = coef;
+                        c.face = f;
+                        c.pad = 0;
+                        const int64_t key = d.idx(i, j, k) * 8 + comp;
+                        auto it = per.find(key);
+                        if (it == per.end()) { keys.push_back(key); per[key].push_back(c); }
+                        else it->second.push_back(c);
+                    }
+            }
+        }
+        std::vector<InjTarget> tg;
+        std::vector<InjContrib> ct;
+        for (int64_t key : keys) {
+            const std::vector<InjContrib> &v = per[key];
+            InjTarget t;
+            t.idx = key / 8; t.comp = (int)(key % 8); t.start = (int32_t)ct.size(); t.count = (int32_t)v.size();
+            t.face = v[0].face;
+            tg.push_back(t);
+            ct.insert(ct.end(), v.begin(), v.end());
+        }
+        const int side = isH;  // d_tg[0] = E targets, d_tg[1] = H targets
+        g->ntg[side] = (int)tg.size();
+        if ((s = dalloc(g, (void **)&g->d_tg[side], tg.size() * sizeof(InjTarget)))) return s;
+        if ((s = dalloc(g, (void **)&g->d_ct[side], ct.size() * sizeof(InjContrib)))) return s;
+        if ((s = upload_raw(g, g->d_tg[side], tg.data(), tg.size() * sizeof(InjTarget)))) return s;
+        if ((s = upload_raw(g, g->d_ct[side], ct.data(), ct.size() * sizeof(InjContrib)))) return s;
+    }
+    // incident tables, TF_SF.cpp:898-955
+    const int Nt = p->Nt;
+    g->einc.assign(Nt + 1, 0.0);
+    g->hinc.assign(Nt + 1, 0.0);
+    const double nu = kC / p->lambda, T = 1.0 / nu;
+    const int nT = (int)(T / dt);
+    const double dnu = kC / (p->lambda - p->dlambda / 2.0) - kC / (p->lambda + p->dlambda / 2.0);
+    const double domega = 2.0 * kPi * dnu;
+    const double sig = domega * domega / (16 * log(2));
+    if (p->cwmode) {
+        const int nd = 5 * nT;
+        for (int n = 0; n < nd && n <= Nt; ++n) {
+            g->einc[n] = exp(-((n * dt) - 5.0 * T) * ((n * dt) - 5 * T) / (4.0 * T * T)) * sin(2.0 * kPi * nu * (n * dt));
+            g->hinc[n] = exp(-((n * dt + dt / 2.0) - 5.0 * T) * ((n * dt + dt / 2.0) - 5 * T) / (4.0 * T * T)) * sin(2.0 * kPi * nu * (n * dt + dt / 2.0));
+        }
+        for (int n = nd; n <= Nt; ++n) {
+            g->einc[n] = sin(2.0 * kPi * nu * (n * dt));
+            g->hinc[n] = sin(2.0 * kPi * nu * (n * dt + dt / 2.0));
+        }
+    } else {
+        const double t0 = 5 * T;
+        for (int n = 0; n <= Nt; ++n) {
+            g->einc[n] = exp(-sig * ((double)n * dt - t0) * ((double)n * dt - t0)) * sin(2.0 * kPi * nu * ((double)n * dt - t0));
+            g->hinc[n] = exp(-sig * ((double)n * dt + dt / 2.0 - t0) * ((double)n * dt + dt / 2.0 - t0)) * sin(2.0 * kPi * nu * ((double)n * dt + dt / 2.0 - t0));
+        }
+    }
+    if ((s = dalloc(g, &g->d_einc, (Nt + 2) * g->esz)) || (s = dalloc(g, &g->d_hinc, (Nt + 2) * g->esz))) return s;
+    if ((s = upload_real(g, g->d_einc, g->einc.data(), Nt + 1)) || (s = upload_real(g, g->d_hinc, g->hinc.data(), Nt + 1)))
+        return s;
+    g->tfsf_on = true;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_tfsf_set_tables(cps_grid *g, int32_t n, const double *einc, const double *hinc)
+{
+    REQUIRE(g && einc && hinc, CPS_E_INVALID, "NULL argument");
+    REQUIRE(g->tfsf_on, CPS_E_STATE, "TF/SF is not initialised");
+    REQUIRE(n == g->tp.Nt + 1, CPS_E_INVALID, "tables must hold Nt + 1 values");
+    g->einc.assign(einc, einc + n);
+    g->hinc.assign(hinc, hinc + n);
+    cps_status s = upload_real(g, g->d_einc, einc, n);
+    return s ? s : upload_real(g, g->d_hinc, hinc, n);
+}
+
+extern "C" cps_status cps_tfsf_get_tables(const cps_grid *g, int32_t n, double *einc, double *hinc)
+{
+    REQUIRE(g && einc && hinc, CPS_E_INVALID, "NULL argument");
+    REQUIRE(g->tfsf_on && n == g->tp.Nt + 1, CPS_E_INVALID, "TF/SF not initialised or wrong length");
+    memcpy(einc, g->einc.data(), n * sizeof(double));
+    memcpy(hinc, g->hinc.data(), n * sizeof(double));
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_source_add(cps_grid *g, int32_t comp, int32_t i, int32_t j, int32_t k, const double *wave,
+                                     int32_t nwave)
+{
+    REQUIRE(g && wave, CPS_E_INVALID, "cps_source_add: NULL argument");
+    REQUIRE(comp >= 0 && comp < 6 && nwave >= 1, CPS_E_INVALID, "cps_source_add: bad component or wave length");
+    REQUIRE(i >= 0 && j >= 0 && k >= 0 && i <= g->d.nx && j <= g->d.ny && k <= g->d.nz, CPS_E_INVALID,
+            "cps_source_add: point outside the grid");
+    Src s;
+    s.comp = comp; s.idx = g->d.idx(i, j, k); s.wave.assign(wave, wave + nwave);
+    g->src.push_back(s);
+    g->src_dirty = true;
+    return CPS_OK;
+}
+
+// ================================================================== ports
+
+extern "C" cps_status cps_port_add(cps_grid *g, int32_t npoints, const int32_t *ijk, int32_t *port_id)
+{
+    REQUIRE(g && ijk && port_id, CPS_E_INVALID, "cps_port_add: NULL argument");
+    REQUIRE(npoints >= 1, CPS_E_INVALID, "cps_port_add: a port needs at least one point");
+    PortState P;
+    P.npts = npoints;
+    P.ijk.assign(ijk, ijk + 3 * (size_t)npoints);
+    std::vector<int64_t> idx(npoints);
+    for (int q = 0; q < npoints; ++q) {
+        const int i = ijk[3 * q], j = ijk[3 * q + 1], k = ijk[3 * q + 2];
+        REQUIRE(i >= 0 && j >= 0 && k >= 0 && i <= g->d.nx && j <= g->d.ny && k <= g->d.nz, CPS_E_INVALID,
+                "cps_port_add: point outside the grid");
+        idx[q] = g->d.idx(i, j, k);
+    }
+    cps_status s;
+    if ((s = dalloc(g, (void **)&P.d_idx, npoints * sizeof(int64_t)))) return s;
+    if ((s = upload_raw(g, P.d_idx, idx.data(), npoints * sizeof(int64_t)))) return s;
+    P.slots = 1;
+    if ((s = dalloc(g, &P.d_ring, (size_t)P.slots * 6 * npoints * g->esz))) return s;
+    g->ports.push_back(P);
+    *port_id = (int32_t)g->ports.size() - 1;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_port_set_dft(cps_grid *g, int32_t port_id, int32_t nfreq, const double *freq_hz,
+                                       uint32_t comp_mask)
+{
+    REQUIRE(g && freq_hz, CPS_E_INVALID, "cps_port_set_dft: NULL argument");
+    REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_set_dft: no such port");
+    REQUIRE(nfreq >= 1 && nfreq <= 4096 && (comp_mask & 63u), CPS_E_INVALID, "cps_port_set_dft: 1..4096 frequencies and a component");
+    PortState &P = g->ports[port_id];
+    REQUIRE(P.nfreq == 0, CPS_E_STATE, "cps_port_set_dft: DFT already configured");
+    P.nfreq = nfreq;
+    P.mask = comp_mask & 63u;
+    P.ncomp = 0;
+    for (int c = 0; c < 6; ++c)
+        if (P.mask & (1u << c)) P.comps[P.ncomp++] = c;
+    std::vector<double> om(nfreq);
+    for (int f = 0; f < nfreq; ++f) om[f] = 2.0 * kPi * freq_hz[f];
+    cps_status s;
+    if ((s = dalloc(g, (void **)&P.d_omega, nfreq * sizeof(double)))) return s;
+    if ((s = upload_raw(g, P.d_omega, om.data(), nfreq * sizeof(double)))) return s;
+    if ((s = dalloc(g, (void **)&P.d_comps, 6 * sizeof(int32_t)))) return s;
+    if ((s = upload_raw(g, P.d_comps, P.comps, 6 * sizeof(int32_t)))) return s;
+    if ((s = dalloc(g, (void **)&P.d_acc, (size_t)P.ncomp * nfreq * 2 * P.npts * sizeof(double)))) return s;
+    // a ring of 64 samples between contractions
+    dfree(g, P.d_ring);
+    P.slots = 64;
+    P.fill = 0;
+    P.last_slot = -1;
+    if ((s = dalloc(g, &P.d_ring, (size_t)P.slots * 6 * P.npts * g->esz))) return s;
+    return CPS_OK;
+}
+
+namespace {
+template <typename T>
+cps_status port_read_T(cps_grid *g, PortState &P, double *out)
+{
+    std::vector<T> tmp((size_t)6 * P.npts, T(0));
+    if (P.last_slot >= 0)
+        CK(cudaMemcpyAsync(tmp.data(), (T *)P.d_ring + (int64_t)P.last_slot * 6 * P.npts, tmp.size() * sizeof(T),
+                           cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    for (int p = 0; p < P.npts; ++p)
+        for (int c = 0; c < 6; ++c) out[p * 6 + c] = (double)tmp[(size_t)c * P.npts + p];
+    return CPS_OK;
+}
+}  // namespace
+
+extern "C" cps_status cps_port_read(cps_grid *g, int32_t port_id, double *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "cps_port_read: NULL argument");
+    REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_read: no such port");
+    PortState &P = g->ports[port_id];
+    return g->fp32 ? port_read_T<float>(g, P, out) : port_read_T<double>(g, P, out);
+}
+
+extern "C" cps_status cps_port_dft_read(cps_grid *g, int32_t port_id, double *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "cps_port_dft_read: NULL argument");
+    REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_dft_read: no such port");
+    PortState &P = g->ports[port_id];
+    REQUIRE(P.nfreq > 0, CPS_E_STATE, "cps_port_dft_read: no DFT configured on this port");
+    cps_status s = flush_dft(g, P);
+    if (s) return s;
+    CK(cudaMemcpyAsync(out, P.d_acc, (size_t)P.ncomp * P.nfreq * 2 * P.npts * sizeof(double), cudaMemcpyDeviceToHost,
+                       g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_port_flux(cps_grid *g, int32_t port_id, char normal, double *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "cps_port_flux: NULL argument");
+    REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_flux: no such port");
+    PortState &P = g->ports[port_id];
+    REQUIRE(P.nfreq > 0, CPS_E_STATE, "cps_port_flux: no DFT configured on this port");
+    int a, b, c, e;  // flux = Re(E_a H_b* - E_c H_e*)
+    double dA;
+    if (normal == 'x') { a = CPS_EY; b = CPS_HZ; c = CPS_EZ; e = CPS_HY; dA = g->desc.dy * g->desc.dz; }
+    else if (normal == 'y') { a = CPS_EZ; b = CPS_HX; c = CPS_EX; e = CPS_HZ; dA = g->desc.dx * g->desc.dz; }
+    else if (normal == 'z') { a = CPS_EX; b = CPS_HY; c = CPS_EY; e = CPS_HX; dA = g->desc.dx * g->desc.dy; }
+    else REQUIRE(false, CPS_E_INVALID, "cps_port_flux: normal must be 'x', 'y' or 'z'");
+    int sel[4], want[4] = {a, b, c, e};
+    for (int q = 0; q < 4; ++q) {
+        sel[q] = -1;
+        for (int ci = 0; ci < P.ncomp; ++ci)
+            if (P.comps[ci] == want[q]) sel[q] = ci;
+        REQUIRE(sel[q] >= 0, CPS_E_STATE, "cps_port_flux: the DFT lacks a tangential component");
+    }
+    cps_status s = flush_dft(g, P);
+    if (s) return s;
+    double *d_out = nullptr;
+    if ((s = dalloc(g, (void **)&d_out, P.nfreq * sizeof(double)))) return s;
+    launch_port_flux(P.d_acc, P.npts, P.nfreq, P.ncomp, sel, dA, d_out, g->stream);
+    g->launches++;
+    cudaError_t e1 = cudaMemcpyAsync(out, d_out, P.nfreq * sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+    cudaError_t e2 = cudaStreamSynchronize(g->stream);
+    dfree(g, d_out);
+    REQUIRE(e1 == cudaSuccess && e2 == cudaSuccess, CPS_E_CUDA, "cps_port_flux: copy failed");
+    return CPS_OK;
+}
+
+// ================================================================== steps
+
+extern "C" cps_status cps_grid_set_step(cps_grid *g, int64_t n)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    g->step = n;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_get_step(const cps_grid *g, int64_t *n)
+{
+    REQUIRE(g && n, CPS_E_INVALID, "NULL argument");
+    *n = g->step;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    REQUIRE(nsteps >= 0, CPS_E_INVALID, "cps_step: negative step count");
+    REQUIRE(path == CPS_PATH_PLAIN || path == CPS_PATH_FUSED, CPS_E_INVALID, "cps_step: unknown path");
+    CK(cudaSetDevice(g->desc.device));
+    return g->fp32 ? step_T<float>(g, nsteps, path) : step_T<double>(g, nsteps, path);
+}
+
+#define OP_BODY(stmt)                                                                              \
+    cps_status s = need_setup(g);                                                                  \
+    if (s) return s;                                                                               \
+    if (g->fp32) { using T = float; stmt; } else { using T = double; stmt; }                       \
+    g->launches++;                                                                                 \
+    return cudaGetLastError() == cudaSuccess ? CPS_OK : (set_error("kernel launch failed"), CPS_E_CUDA);
+
+extern "C" cps_status cps_op_h_bulk(cps_grid *g) { OP_BODY(launch_h_bulk<T>(field_view<T>(g), g->stream)) }
+extern "C" cps_status cps_op_e_bulk(cps_grid *g) { OP_BODY(launch_e_bulk<T>(field_view<T>(g), g->stream)) }
+extern "C" cps_status cps_op_h_pml(cps_grid *g)
+{
+    if (g && !g->pml_on) { set_error("CPML not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_h_pml<T>(field_view<T>(g), pml_view<T>(g), g->stream))
+}
+extern "C" cps_status cps_op_e_pml(cps_grid *g)
+{
+    if (g && !g->pml_on) { set_error("CPML not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_e_pml<T>(field_view<T>(g), pml_view<T>(g), g->stream))
+}
+extern "C" cps_status cps_op_dl(cps_grid *g)
+{
+    if (g && !g->dl_on) { set_error("Drude-Lorentz not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_dl<T>(field_view<T>(g), dl_view<T>(g), g->stream))
+}
+extern "C" cps_status cps_op_gain_polarization(cps_grid *g)
+{
+    if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 0, g->stream))
+}
+extern "C" cps_status cps_op_gain_efield(cps_grid *g)
+{
+    if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 1, g->stream))
+}
+extern "C" cps_status cps_op_gain_populations(cps_grid *g)
+{
+    if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
+    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 2, g->stream))
+}
+extern "C" cps_status cps_op_tfsf_h(cps_grid *g, int32_t n, uint32_t face_mask)
+{
+    if (g && !g->tfsf_on) { set_error("TF/SF not initialised"); return CPS_E_STATE; }
+    OP_BODY(op_inject<T>(g, 1, (double)n, face_mask))
+}
+extern "C" cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask)
+{
+    if (g && !g->tfsf_on) { set_error("TF/SF not initialised"); return CPS_E_STATE; }
+    OP_BODY(op_inject<T>(g, 0, (double)n, face_mask))
+}
+extern "C" cps_status cps_op_sources(cps_grid *g, int32_t n)
+{
+    if (g) { cps_status s0 = ensure_sources(g); if (s0) return s0; }
+    OP_BODY(op_sources<T>(g, n))
+}
+extern "C" cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n)
+{
+    if (g && (port_id < 0 || port_id >= (int)g->ports.size())) { set_error("no such port"); return CPS_E_NOTFOUND; }
+    OP_BODY(if (op_port<T>(g, g->ports[port_id], n)) return CPS_E_CUDA)
+}
+
+// ============================================================ field access
+
+namespace {
+template <typename T>
+cps_status download_T(cps_grid *g, int comp, double *out)
+{
+    const size_t n = (size_t)(g->d.nx + 1) * (g->d.ny + 1) * (g->d.nz + 1);
+    if (!g->d_conv) {
+        cps_status s = dalloc(g, (void **)&g->d_conv, n * sizeof(double));
+        if (s) return s;
+    }
+    launch_from_device_layout<T>((const T *)g->F[comp], g->d_conv, g->d, g->stream);
+    CK(cudaMemcpyAsync(out, g->d_conv, n * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+template <typename T>
+cps_status upload_field_T(cps_grid *g, int comp, const double *in)
+{
+    const size_t n = (size_t)(g->d.nx + 1) * (g->d.ny + 1) * (g->d.nz + 1);
+    if (!g->d_conv) {
+        cps_status s = dalloc(g, (void **)&g->d_conv, n * sizeof(double));
+        if (s) return s;
+    }
+    CK(cudaMemcpyAsync(g->d_conv, in, n * sizeof(double), cudaMemcpyHostToDevice, g->stream));
+    launch_to_device_layout<T>(g->d_conv, (T *)g->F[comp], g->d, g->stream);
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+}  // namespace
+
+extern "C" cps_status cps_field_download(cps_grid *g, int32_t comp, double *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "cps_field_download: NULL argument");
+    REQUIRE(comp >= 0 && comp < 6, CPS_E_INVALID, "cps_field_download: component 0..5");
+    return g->fp32 ? download_T<float>(g, comp, out) : download_T<double>(g, comp, out);
+}
+
+extern "C" cps_status cps_field_upload(cps_grid *g, int32_t comp, const double *in)
+{
+    REQUIRE(g && in, CPS_E_INVALID, "cps_field_upload: NULL argument");
+    REQUIRE(comp >= 0 && comp < 6, CPS_E_INVALID, "cps_field_upload: component 0..5");
+    return g->fp32 ? upload_field_T<float>(g, comp, in) : upload_field_T<double>(g, comp, in);
+}
+
+extern "C" cps_status cps_field_download_f32(cps_grid *g, int32_t comp, float *out)
+{
+    REQUIRE(g && out, CPS_E_INVALID, "NULL argument");
+    REQUIRE(comp >= 0 && comp < 6, CPS_E_INVALID, "component 0..5");
+    const size_t n = (size_t)(g->d.nx + 1) * (g->d.ny + 1) * (g->d.nz + 1);
+    std::vector<double> tmp(n);
+    cps_status s = cps_field_download(g, comp, tmp.data());
+    if (s) return s;
+    for (size_t q = 0; q < n; ++q) out[q] = (float)tmp[q];
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    for (int c = 0; c < 6; ++c) CK(cudaMemsetAsync(g->F[c], 0, (size_t)g->elems * g->esz, g->stream));
+    if (g->pml_on) {
+        const Dims &d = g->d;
+        for (int f = 0; f < 6; ++f) {
+            const int np = g->pml.npml[f];
+            size_t n;
+            if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * (np + 1);
+            else if (f < 4) n = (size_t)(d.nz + 1) * (np + 1) * d.px;
+            else n = (size_t)(np + 1) * (d.ny + 1) * d.px;
+            for (int q = 0; q < 4; ++q) CK(cudaMemsetAsync(g->d_q[f][q], 0, n * g->esz, g->stream));
+        }
+    }
+    if (g->dl_on) CK(cudaMemsetAsync(g->d_dl_state, 0, (size_t)g->dl_n * 3 * g->dlc.stride * g->esz, g->stream));
+    if (g->gain_on) {
+        std::vector<double> init;
+        gain_initial_state(g, init, g->g_n);
+        cps_status s = upload_real(g, g->d_g_state, init.data(), init.size());
+        if (s) return s;
+    }
+    for (PortState &P : g->ports) {
+        P.fill = 0;
+        P.last_slot = -1;
+        CK(cudaMemsetAsync(P.d_ring, 0, (size_t)P.slots * 6 * P.npts * g->esz, g->stream));
+        if (P.d_acc) CK(cudaMemsetAsync(P.d_acc, 0, (size_t)P.ncomp * P.nfreq * 2 * P.npts * sizeof(double), g->stream));
+    }
+    g->step = n0;
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_check_finite(cps_grid *g, int64_t *nonfinite)
+{
+    REQUIRE(g && nonfinite, CPS_E_INVALID, "NULL argument");
+    CK(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned long long), g->stream));
+    if (g->fp32) launch_count_nonfinite<float>(field_view<float>(g), g->d_counter, g->stream);
+    else launch_count_nonfinite<double>(field_view<double>(g), g->d_counter, g->stream);
+    g->launches++;
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, g->d_counter, sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    *nonfinite = (int64_t)h;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *ncells)
+{
+    REQUIRE(g && ncells, CPS_E_INVALID, "NULL argument");
+    REQUIRE(g->gain_on, CPS_E_STATE, "gain not initialised");
+    *ncells = g->g_n;
+    if (!out) return CPS_OK;
+    const int nw = g->fp32 ? kG32Words : kG64Words;
+    const size_t n = (size_t)g->g_n * nw;
+    std::vector<double> st(n);
+    if (g->fp32) {
+        std::vector<float> t(n);
+        CK(cudaMemcpyAsync(t.data(), g->d_g_state, n * 4, cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+        for (size_t q = 0; q < n; ++q) st[q] = t[q];
+    } else {
+        CK(cudaMemcpyAsync(st.data(), g->d_g_state, n * 8, cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+    }
+    // device list is in device order (k, j, i); report in (i, j, k) order
+    std::vector<int64_t> cells(g->g_n);
+    CK(cudaMemcpy(cells.data(), g->d_g_cell, g->g_n * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    std::vector<std::pair<int64_t, int64_t>> ord(g->g_n);
+    const Dims &d = g->d;
+    for (int64_t c = 0; c < g->g_n; ++c) {
+        const int64_t q = cells[c];
+        const int k = (int)(q / d.pxy), j = (int)((q - k * d.pxy) / d.px), i = (int)(q - k * d.pxy - (int64_t)j * d.px);
+        ord[c] = {((int64_t)i * (d.ny + 1) + j) * (d.nz + 1) + k, c};
+    }
+    std::sort(ord.begin(), ord.end());
+    const int64_t sc = g->g_n;
+    for (int64_t r = 0; r < g->g_n; ++r) {
+        const int64_t c = ord[r].second;
+        double N[4];
+        if (g->fp32) {
+            N[1] = 1.0 + st[12 * sc + c]; N[2] = st[13 * sc + c]; N[3] = st[14 * sc + c];
+            N[0] = 2.0 - N[1] - N[2] - N[3];
+        } else {
+            for (int q = 0; q < 4; ++q) N[q] = st[(21 + q) * sc + c];
+        }
+        for (int q = 0; q < 4; ++q) out[r * 4 + q] = N[q];
+    }
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_launch_count(const cps_grid *g, int64_t *launches)
+{
+    REQUIRE(g && launches, CPS_E_INVALID, "NULL argument");
+    *launches = g->launches;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_ports_flush(cps_grid *g)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    for (PortState &P : g->ports) {
+        cps_status s = flush_dft(g, P);
+        if (s) return s;
+    }
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_set_timing(cps_grid *g, int32_t stride)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    REQUIRE(stride >= 0, CPS_E_INVALID, "cps_grid_set_timing: negative stride");
+    CK(cudaStreamSynchronize(g->stream));
+    if (g->ev.empty() && stride > 0) {
+        g->ev.resize(4 * 4096);
+        for (auto &e : g->ev) CK(cudaEventCreate(&e));
+    }
+    g->timing_stride = stride;
+    g->ev_used = 0;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_timing(cps_grid *g, double *h_ms, double *e_ms, int64_t *samples)
+{
+    REQUIRE(g && h_ms && e_ms && samples, CPS_E_INVALID, "NULL argument");
+    CK(cudaStreamSynchronize(g->stream));
+    double h = 0, e = 0;
+    const int n = g->ev_used / 4;
+    for (int s = 0; s < n; ++s) {
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, g->ev[4 * s], g->ev[4 * s + 1]));
+        CK(cudaEventElapsedTime(&b, g->ev[4 * s + 2], g->ev[4 * s + 3]));
+        h += a;
+        e += b;
+    }
+    *h_ms = n ? h / n : 0.0;
+    *e_ms = n ? e / n : 0.0;
+    *samples = n;
+    return CPS_OK;
+}

@@ -1,0 +1,156 @@
+// cells.cuh -- per-cell recursions shared by the plain and fused kernels.
+//
+// Each function is the device form of one reference update at one cell; the
+// arithmetic keeps the reference's operation order term by term.
+#pragma once
+
+#include "cps_internal.h"
+
+namespace cps {
+
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+// One component of the Drude-Lorentz ADE at one cell: Drude_Lorentz.cpp:163-184.
+// curl is the curl term already multiplied by C3; the state words of this
+// component are st[w * stride_cells], w = JD[nD] JL[nL] JL1[nL] E1.
+template <typename T>
+__device__ __forceinline__ T dl_component(const DlCoef<T> &D, T E, T curl, T *st, int64_t sc)
+{
+    const T temp = E;
+    T t1 = T(0), t2 = T(0);
+#pragma unroll 1
+    for (int p = 0; p < D.nD; ++p) t1 = t1 + D.C4[p] * st[p * sc];
+#pragma unroll 1
+    for (int p = 0; p < D.nL; ++p) t2 = t2 + D.C5[p] * st[(D.nD + p) * sc] + D.C6[p] * st[(D.nD + D.nL + p) * sc];
+    T *E1 = st + (D.nD + 2 * D.nL) * sc;
+    const T e1 = *E1;
+    E = D.C1 * E + D.C2 * e1 + curl - t1 - t2;
+#pragma unroll 1
+    for (int p = 0; p < D.nD; ++p) st[p * sc] = D.kappa[p] * st[p * sc] + D.beta[p] * (E + temp);
+#pragma unroll 1
+    for (int p = 0; p < D.nL; ++p) {
+        const T t0 = st[(D.nD + p) * sc];
+        st[(D.nD + p) * sc] = D.alpha[p] * t0 + D.xi[p] * st[(D.nD + D.nL + p) * sc] + D.gammaL[p] * (E - e1) / T(2.0) / D.dt;
+        st[(D.nD + D.nL + p) * sc] = t0;
+    }
+    *E1 = temp;
+    return E;
+}
+
+// ---------------------------------------------------------------- gain
+// FP64 layout (reference state, unscaled): words
+//   0..2 Pa, 3..5 Pa1, 6..8 Pa2, 9..11 Pb, 12..14 Pb1, 15..17 Pb2, 18..20 E1, 21..24 N0..N3
+// FP32 layout (P scaled by CEP, populations as offsets): words
+//   0..2 Pa, 3..5 Pa1, 6..8 Pb, 9..11 Pb1, 12 N1-1, 13 N2, 14 N3, 15..17 Pa2, 18..20 Pb2, 21..23 E1
+struct GainSite64 {
+    static constexpr int PA = 0, PA1 = 3, PA2 = 6, PB = 9, PB1 = 12, PB2 = 15, E1 = 18, N = 21;
+};
+struct GainSite32 {
+    static constexpr int PA = 0, PA1 = 3, PB = 6, PB1 = 9, DN1 = 12, N2 = 13, N3 = 14, PA2 = 15, PB2 = 18, E1 = 21;
+};
+
+// populations of a site as FP64 N0..N3
+template <typename T>
+__device__ __forceinline__ void gain_load_n(const T *st, int64_t sc, double N[4]);
+template <>
+__device__ __forceinline__ void gain_load_n<double>(const double *st, int64_t sc, double N[4])
+{
+    for (int q = 0; q < 4; ++q) N[q] = st[(GainSite64::N + q) * sc];
+}
+template <>
+__device__ __forceinline__ void gain_load_n<float>(const float *st, int64_t sc, double N[4])
+{
+    N[1] = 1.0 + (double)st[GainSite32::DN1 * sc];
+    N[2] = (double)st[GainSite32::N2 * sc];
+    N[3] = (double)st[GainSite32::N3 * sc];
+    N[0] = 2.0 - N[1] - N[2] - N[3];  // FP64 conservation, FourLevelLaser.cpp:324
+}
+
+// P update (FourLevelLaser.cpp:274-295) with explicit P, P1 in/out and the
+// shifted-out P2 returned; P values are in the grid's storage scale.
+template <typename T>
+__device__ __forceinline__ void gain_p_update(const GainCoef &G, const double N[4], const T E[3], T Pa[3],
+                                              T Pa1[3], T Pa2[3], T Pb[3], T Pb1[3], T Pb2[3])
+{
+    const T ca1 = (T)G.CPa1, ca2 = (T)G.CPa2, ca3 = (T)(G.CPa3 * G.scaleP);
+    const T cb1 = (T)G.CPb1, cb2 = (T)G.CPb2, cb3 = (T)(G.CPb3 * G.scaleP);
+    const T dNa = (T)(N[2] - N[1]), dNb = (T)(N[3] - N[0]);
+    for (int c = 0; c < 3; ++c) {
+        Pa2[c] = Pa1[c];
+        Pa1[c] = Pa[c];
+        Pa[c] = ca1 * Pa[c] + ca2 * Pa2[c] + E[c] * ca3 * dNa;
+    }
+    for (int c = 0; c < 3; ++c) {
+        Pb2[c] = Pb1[c];
+        Pb1[c] = Pb[c];
+        Pb[c] = cb1 * Pb[c] + cb2 * Pb2[c] + E[c] * cb3 * dNb;
+    }
+}
+
+// E correction (FourLevelLaser.cpp:302-305): E -= CEP (dPa + dPb)
+template <typename T>
+__device__ __forceinline__ T gain_e_corr(const GainCoef &G, T E, T pa, T pa1, T pb, T pb1)
+{
+    if (G.scaleP == 1.0) return E - (T)G.CEP * (pa - pa1 + pb - pb1);
+    return E - (pa - pa1 + pb - pb1);  // P already carries the factor CEP
+}
+
+// Population update (FourLevelLaser.cpp:313-324) in FP64; the N2 term for Ey
+// uses Pay - Pay_1 as the reference does (:316), Ez follows the Ex form; the
+// pump moves pump_rate*dt*N0 from N0 to N3.
+template <typename T>
+__device__ __forceinline__ void gain_n_update(const GainCoef &G, double N[4], const T E[3], const T E1[3],
+                                              const T Pa[3], const T Pa1[3], const T Pa2[3], const T Pb[3],
+                                              const T Pb2[3])
+{
+    const double inv = 1.0 / G.scaleP;
+    // on FP64 grids (scaleP == 1) the sums keep the reference's exact roundings
+    double sb = (double)E1[0] * ((double)Pb[0] - (double)Pb2[0]) + (double)E1[1] * ((double)Pb[1] - (double)Pb2[1]);
+    sb = sb + (double)E1[2] * ((double)Pb[2] - (double)Pb2[2]);
+    if (G.scaleP != 1.0) sb = sb * inv;
+    const double N0old = N[0];
+    N[3] = G.t30t32dt / (G.t30t32_2 + G.t30dt * (1 - N[2]) + G.t32dt * (1 - N[0])) *
+           (N[3] * ((N[0] - 1) / G.t30 + (N[2] - 1) / G.t32 + G.dt_2) + sb / G.homega_bdt);
+    N[3] = N[3] + G.pump_dt * N0old;
+    double sa = (double)E1[0] * ((double)Pa[0] - (double)Pa2[0]) + (double)E1[1] * ((double)Pa[1] - (double)Pa2[1]);
+    sa = sa + (double)E1[2] * ((double)Pa[2] - (double)Pa2[2]);
+    double s2 = ((double)E[0] + (double)E1[0]) * ((double)Pa[0] - (double)Pa2[0]) + ((double)E[1] + (double)E1[1]) * ((double)Pa[1] - (double)Pa1[1]);
+    s2 = s2 + ((double)E[2] + (double)E1[2]) * ((double)Pa[2] - (double)Pa2[2]);
+    if (G.scaleP != 1.0) { sa = sa * inv; s2 = s2 * inv; }
+    N[1] = G.t10t21dt / (G.t10t21_2 + G.t10dt * N[2] + G.t21dt * (1 - N[0])) *
+           (N[1] * ((N[0] - 1) / G.t10 - N[2] / G.t21 + G.dt_2) + N[2] / G.t21_2 - sa / G.homega_adt);
+    N[2] = G.t32t21dt / (G.t32t21_2 + G.t21dt * N[3] + G.t32dt * (1 - N[1])) *
+           (N[2] * ((N[1] - 1) / G.t21 - N[3] / G.t32 + G.dt_2) + N[3] / G.t32_2 + s2 / G.homega_adt);
+    N[0] = 2.0 - N[1] - N[2] - N[3];
+}
+
+template <typename T>
+__device__ __forceinline__ void gain_store_n(T *st, int64_t sc, const double N[4]);
+template <>
+__device__ __forceinline__ void gain_store_n<double>(double *st, int64_t sc, const double N[4])
+{
+    for (int q = 0; q < 4; ++q) st[(GainSite64::N + q) * sc] = N[q];
+}
+template <>
+__device__ __forceinline__ void gain_store_n<float>(float *st, int64_t sc, const double N[4])
+{
+    st[GainSite32::DN1 * sc] = (float)(N[1] - 1.0);
+    st[GainSite32::N2 * sc] = (float)N[2];
+    st[GainSite32::N3 * sc] = (float)N[3];
+}
+
+// TF/SF incident-table lookup, TF_SF.cpp:966-986; indices past the table read 0
+template <typename T>
+__device__ __forceinline__ double inc_lookup(const T *tab, int Nt, double retarded)
+{
+    if (retarded <= 0) return 0.0;
+    const double fl = floor(retarded);
+    const double resid = retarded - fl;
+    const long long m = (long long)fl;
+    const double a = m <= Nt ? (double)tab[m] : 0.0;
+    const double b = m + 1 <= Nt ? (double)tab[m + 1] : 0.0;
+    return ((1.0 - resid) * a + resid * b);
+}
+
+}  // namespace cps

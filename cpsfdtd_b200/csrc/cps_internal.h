@@ -1,0 +1,179 @@
+// cps_internal.h -- device layout and kernel interfaces of the engine.
+//
+// Device layout of a grid with nx*ny*nz cells (reference arrays span 0..N):
+//   every field and the uint8 material-ID array is NX*NY*NZ values with
+//   NX = nx+1 padded to `px` (a multiple of 32), NY = ny+1, NZ = nz+1,
+//   linear index i + px*(j + NY*k): x fastest, so a warp reads 32
+//   consecutive cells of one row and a thread marching in k walks a column.
+//   CPML psi lives only on the six boundary slabs; Drude-Lorentz and gain
+//   state only on compacted cell lists sorted by linear index (SoA, one array
+//   per state word), found from a thread's cell by a per-warp-segment start
+//   offset and a ballot rank.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cps_capi.h"
+
+namespace cps {
+
+constexpr int kXPad = 32;
+constexpr int kMaxPoles = CPS_MAX_POLES;
+constexpr int kFX1 = 0, kFX2 = 1, kFY1 = 2, kFY2 = 3, kFZ1 = 4, kFZ2 = 5;
+
+// Physical constants, values as Constants.h:19-26
+constexpr double kPi = 3.1415926535897932384626433832795;
+constexpr double kC = 2.99792458E8;
+constexpr double kHPlanck = 6.62607004081E-34;
+constexpr double kMu0 = 1.2566370614E-6;
+constexpr double kEps0 = 8.8541878176E-12;
+
+struct Dims {
+    int nx, ny, nz;   // cells
+    int px;           // x pitch in elements
+    int64_t pxy;      // px * (ny+1): plane stride
+    __host__ __device__ int64_t idx(int i, int j, int k) const
+    {
+        return (int64_t)i + (int64_t)px * j + pxy * k;
+    }
+};
+
+// --- Drude-Lorentz coefficients (host FP64, converted to T for the device)
+template <typename T>
+struct DlCoef {
+    int nD, nL, stride;  // stride = words per component = nD + 2 nL + 1
+    T C1, C2, C3, dt, inv2dt;
+    T kappa[kMaxPoles], beta[kMaxPoles], C4[kMaxPoles];
+    T alpha[kMaxPoles], xi[kMaxPoles], gammaL[kMaxPoles], C5[kMaxPoles], C6[kMaxPoles];
+};
+
+// --- gain coefficients.  FP64 grids hold P unscaled (scaleP = 1); FP32 grids
+// hold P multiplied by CEP so that it stays in the normal float range, and
+// populations as offsets from their initial values (N1-1, N2, N3).
+struct GainCoef {
+    double CPa1, CPa2, CPa3, CPb1, CPb2, CPb3, CEP;
+    double t30, t32, t21, t10;
+    double t30t32dt, t30t32_2, t30dt, t32dt, dt_2, homega_bdt;
+    double t10t21dt, t10t21_2, t10dt, t21dt, t21_2, homega_adt;
+    double t32t21dt, t32t21_2, t32_2;
+    double pump_dt;
+    double scaleP;  // P stored = scaleP * P
+};
+
+// per-cell gain state words
+constexpr int kG64Words = 25;  // Pa Pa1 Pa2 Pb Pb1 Pb2 (x3 each) E1 (x3) N0..N3
+constexpr int kG32Words = 24;  // Pa Pa1 Pb Pb1 (x3, scaled) dN1 N2 N3 | Pa2 Pb2 E1 (x3, per-routine transients)
+
+// --- TF/SF / source injection in CSR form: each target (cell, component)
+// owns a run of contributions applied in the reference's face order.
+struct InjTarget {
+    int64_t idx;
+    int32_t comp;
+    int32_t start;
+    int32_t count;
+    int32_t face;  // face of the first contribution (for face-mask calls)
+};
+struct InjContrib {
+    double delay;    // retarded-time offset in steps (k.r/c - l0)/dt
+    double profile;  // Gaussian transverse profile
+    double coef;     // signed C * E0/H0 component
+    int32_t face;
+    int32_t pad;
+};
+
+template <typename T>
+struct PmlView {
+    int on;
+    int np[6];
+    const T *bE[6], *cE[6], *bH[6], *cH[6];
+    T *qe[6][2], *qh[6][2];  // x slabs [k][j][s], y slabs [k][s][i], z slabs [s][j][i]
+    T cpmlE, cpmlH;
+};
+
+template <typename T>
+struct StretchView {
+    // names as Structure.h:82-83
+    const T *cExy, *cEyx, *cEzx, *cExz, *cEzy, *cEyz;
+    const T *cHxy, *cHyx, *cHzx, *cHxz, *cHzy, *cHyz;
+};
+
+template <typename T>
+struct FieldView {
+    Dims d;
+    T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    const uint8_t *id;
+    const T *aE, *bE, *aH, *bH;  // 256 entries each
+    StretchView<T> s;
+};
+
+template <typename T>
+struct DlView {
+    int on;
+    int64_t ncell;
+    const int64_t *cell;     // sorted linear indices
+    const int32_t *seg;      // start offset per (k, j, 32-wide x segment)
+    T *state;                // [word][ncell]
+    DlCoef<T> c;
+};
+
+template <typename T>
+struct GainView {
+    int on;
+    int gain_id;
+    int64_t ncell;
+    const int64_t *cell;
+    const int32_t *seg;
+    T *state;                // [word][ncell]
+    GainCoef c;
+};
+
+// ------------------------------------------------------------ launchers
+// Plain path: one kernel per reference routine (kernels_plain.cu, built
+// without FMA contraction so FP64 results follow the reference roundings).
+template <typename T> void launch_h_bulk(const FieldView<T> &f, cudaStream_t s);
+template <typename T> void launch_e_bulk(const FieldView<T> &f, cudaStream_t s);
+template <typename T> void launch_h_pml(const FieldView<T> &f, const PmlView<T> &p, cudaStream_t s);
+template <typename T> void launch_e_pml(const FieldView<T> &f, const PmlView<T> &p, cudaStream_t s);
+template <typename T> void launch_dl(const FieldView<T> &f, const DlView<T> &d, cudaStream_t s);
+template <typename T> void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStream_t s);
+template <typename T>
+void launch_inject(const FieldView<T> &f, const InjTarget *tg, int ntarget, const InjContrib *ct,
+                   const T *table, int Nt, double n, uint32_t face_mask, cudaStream_t s);
+template <typename T>
+void launch_sources(const FieldView<T> &f, int nsrc, const int64_t *idx, const int32_t *comp,
+                    const double *waves, const int32_t *wave_off, const int32_t *wave_len, int n,
+                    cudaStream_t s);
+
+// Fused path (kernels_fused.cu): 2.5D z-marching sweeps.
+struct FusedShape {
+    int by;   // rows per block (block = 32 x by threads)
+    int kc;   // planes per block along z
+};
+template <typename T>
+void launch_h_fused(const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, cudaStream_t s);
+template <typename T>
+void launch_e_fused(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &d,
+                    const GainView<T> &g, FusedShape sh, cudaStream_t s);
+
+// Ports (kernels_ports.cu)
+template <typename T>
+void launch_port_gather(const FieldView<T> &f, const int64_t *idx, int npts, T *ring_slot,
+                        cudaStream_t s);
+template <typename T>
+void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, double dt,
+                     const double *omega, int nfreq, const int32_t *comps, int ncomp,
+                     double *acc, double *scratch_phasor, cudaStream_t s);
+void launch_port_flux(const double *acc, int npts, int nfreq, int ncomp, const int32_t *sign_pair,
+                      double dA, double *out, cudaStream_t s);
+template <typename T>
+void launch_count_nonfinite(const FieldView<T> &f, unsigned long long *out, cudaStream_t s);
+template <typename T>
+void launch_to_device_layout(const double *src, T *dst, Dims d, cudaStream_t s);
+template <typename T>
+void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s);
+
+}  // namespace cps

@@ -1,0 +1,269 @@
+/*
+ * cps_capi.h -- C ABI of the B200 cpsFDTD time-stepping engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a cps_status
+ * (0 = success); cps_last_error() returns the message of the last failure on
+ * the calling thread.  A cps_grid is one simulation domain resident on one
+ * GPU; one grid handle must not be used from two threads at once, distinct
+ * grids may be driven concurrently.
+ *
+ * Host-side arrays use the reference's storage order: a field or ID grid is
+ * (nx+1)*(ny+1)*(nz+1) values in [i][j][k] order with k fastest (Fields.cpp:
+ * 101-131).  On the device the engine keeps its own layout (x fastest, rows
+ * padded to 32 elements); copies convert.
+ *
+ * Reference interface each call replaces (file:line inside the cpsFDTD tree):
+ *   cps_grid_create ........... Structure::generate_mesh grid sizing (Structure.cpp:68-157),
+ *                               Field::Field (Fields.cpp:52-186)
+ *   cps_grid_set_media ........ Structure::Structure + InitializeBasicFDTDCoefficients
+ *                               (Structure.cpp:26-52, 309-359)
+ *   cps_grid_upload_ids ....... Structure::ID (Structure.h:36), filled by generate_mesh
+ *   cps_mesh_rasterize ........ cuboid/ellipsoid/cylinder/multishape (Structure.cpp:159-307)
+ *   cps_pml_init .............. CPML::CPML + InitializeCPML (CPML.cpp:29-68, 231-527);
+ *                               CFS_PML::CFS_PML + Initialize_PML (CFS_PML.h:33-36)
+ *   cps_dl_init ............... Drude_Lorentz::Drude_Lorentz (Drude_Lorentz.cpp:30-147)
+ *   cps_gain_init ............. FourLevelLaser::FourLevelLaser (FourLevelLaser.cpp:30-213)
+ *   cps_tfsf_init ............. TF_SF::TF_SF (TF_SF.cpp:29-959)
+ *   cps_source_add ............ the field injection of main.cpp:284-286
+ *   cps_port_points_plain ..... PlainPort::PlainPort point set (Ports.cpp:201-306)
+ *   cps_port_points_spherical . SphericalPort::SphericalPort point set (Ports.cpp:28-86)
+ *   cps_port_add .............. a port's Port_Points array (Ports.h:29-36)
+ *   cps_op_h_bulk / e_bulk .... BasicHFieldUpdate / BasicEFieldUpdate (BasicFDTD.cpp:67-84, 25-47)
+ *   cps_op_h_pml / e_pml ...... CPML::UpdateCPMLHFields / UpdateCPMLEFields (CPML.cpp:609-689,
+ *                               529-607); CFS_PML::UpdatePMLHFields / UpdatePMLEFields
+ *   cps_op_dl ................. Drude_Lorentz::EFieldUpdate (Drude_Lorentz.cpp:153-227), 3-D form
+ *   cps_op_gain_polarization .. FourLevelLaser::UpdatePolarizationDensities (FourLevelLaser.cpp:270-298)
+ *   cps_op_gain_efield ........ FourLevelLaser::UpdateElectricField (FourLevelLaser.cpp:300-308)
+ *   cps_op_gain_populations ... FourLevelLaser::UpdateStatesPopulations (FourLevelLaser.cpp:310-325)
+ *   cps_op_tfsf_h / tfsf_e .... TF_SF::UpdateHField / UpdateEField and the face variants
+ *                               (TF_SF.cpp:1201-1410, 988-1199)
+ *   cps_op_port_sample ........ SphericalPort/PlainPort::Update_Fields_on_Port (Ports.cpp:88-99, 342-353)
+ *   cps_step .................. one pass of the loop body of main.cpp:267-344
+ *   cps_field_download/upload . direct access to Field::Ex..Hz (Fields.h:28-33)
+ *   cps_port_read ............. Port_Points::Ex..Hz after Update_Fields_on_Port
+ *   cps_port_dft_read / flux .. (no reference counterpart: running FP64 DFT of the port samples)
+ */
+#ifndef CPS_CAPI_H
+#define CPS_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define CPS_API __attribute__((visibility("default")))
+#else
+#define CPS_API
+#endif
+
+typedef int32_t cps_status;
+typedef struct cps_grid cps_grid;
+
+enum {
+    CPS_OK = 0,
+    CPS_E_INVALID = 1,   /* bad argument or inconsistent configuration */
+    CPS_E_CUDA = 2,      /* a CUDA call failed */
+    CPS_E_NOMEM = 3,     /* device or host allocation failed */
+    CPS_E_STATE = 4,     /* call not valid in the grid's current state */
+    CPS_E_NUMERIC = 5,   /* non-finite field values detected */
+    CPS_E_BUDGET = 6,    /* memory footprint exceeds the admission budget */
+    CPS_E_TIMEOUT = 7,   /* a bounded device wait gave up */
+    CPS_E_CANCELLED = 8, /* job cancelled */
+    CPS_E_NOTFOUND = 9   /* unknown handle, port or job */
+};
+
+enum { CPS_FP64 = 0, CPS_FP32 = 1 };
+enum { CPS_EX = 0, CPS_EY = 1, CPS_EZ = 2, CPS_HX = 3, CPS_HY = 4, CPS_HZ = 5 };
+/* cps_step paths: PLAIN launches one kernel per reference routine in the
+ * reference order; FUSED runs the fused sweeps (same results within the
+ * precision's tolerance). */
+enum { CPS_PATH_PLAIN = 0, CPS_PATH_FUSED = 1 };
+/* TF/SF face bits for cps_op_tfsf_* (TF_SF.h:41-52 face variants) */
+enum { CPS_FACE_X1 = 1, CPS_FACE_X2 = 2, CPS_FACE_Y1 = 4, CPS_FACE_Y2 = 8,
+       CPS_FACE_Z1 = 16, CPS_FACE_Z2 = 32, CPS_FACE_ALL = 63 };
+
+/* Material IDs with fixed meaning in the E update (BasicFDTD.cpp:34-38) */
+#define CPS_ID_DISPERSIVE 2
+#define CPS_ID_PEC 4
+
+typedef struct cps_grid_desc {
+    int32_t nx, ny, nz;      /* Structure::Nx..Nz; arrays span indices 0..N */
+    double dx, dy, dz;       /* metres */
+    double dt;               /* seconds; 0 selects 0.99 of the Courant limit (Structure.cpp:124) */
+    int32_t precision;       /* CPS_FP64 or CPS_FP32 */
+    int32_t device;          /* CUDA device ordinal */
+} cps_grid_desc;
+
+/* CPML deck values (CPML.cpp:37-62).  npml order x1 x2 y1 y2 z1 z2; both ends
+ * of an axis must be equal and >= 1, or both 0 to leave that axis open. */
+typedef struct cps_pml_params {
+    int32_t npml[6];
+    double m, malp, kapmax, sig_ratio, alpmax;
+} cps_pml_params;
+
+/* Drude-Lorentz deck values (Drude_Lorentz.cpp:37-94); frequencies in Hz.
+ * literal = 1 uses C1 and C5 exactly as Drude_Lorentz.cpp:96,106; 0 uses the
+ * values the ADE discretisation gives (the literal C5 lacks a factor dt and is
+ * unstable with any Lorentz pole). */
+#define CPS_MAX_POLES 8
+typedef struct cps_dl_params {
+    double sigma, epsInf;
+    int32_t nD, nL;
+    double fD[CPS_MAX_POLES], gD[CPS_MAX_POLES];
+    double fL[CPS_MAX_POLES], dL[CPS_MAX_POLES], depsL[CPS_MAX_POLES];
+    int32_t literal;
+} cps_dl_params;
+
+/* Four-level gain deck values (FourLevelLaser.cpp:37-93).  Gain sites are the
+ * cells whose ID equals gain_id (the reference places them on ID==5,
+ * FourLevelLaser.cpp:119-140).  pump_rate (1/s) moves population N0 -> N3 and
+ * has no reference counterpart; 0 reproduces the reference. */
+typedef struct cps_gain_params {
+    int32_t gain_id;
+    double lambda_a, lambda_b, gamma_a, gamma_b;
+    double t30, t32, t21, t10;
+    double N_0;
+    double pump_rate;
+} cps_gain_params;
+
+/* TF/SF deck values (TF_SF.cpp:35-97, 898-907).  i0 = xs/dx and j0 = ys/dy
+ * (truncated), z0 = zs/dz as the reference sets it (TF_SF.cpp:55-57), k0 the
+ * beam-centre plane (TF_SF.h:65; the reference never assigns it).  Angles in
+ * degrees.  n[] = nTFSF x1 x2 y1 y2 z1 z2.  Nt = incident-table length - 1. */
+typedef struct cps_tfsf_params {
+    double lambda, dlambda, w0, z0;
+    int32_t i0, j0, k0;
+    double theta_deg, phi_deg, E0, psi_deg;
+    int32_t n[6];
+    int32_t Nt;
+    int32_t cwmode;
+} cps_tfsf_params;
+
+/* One structure.txt shape line (Structure.cpp:88-106); type 0 cuboid,
+ * 1 ellipsoid, 2 cylinder, 3 multi (theta/phi/psi = counts, a/b/c = pitch,
+ * material_index = index of the template shape). */
+enum { CPS_SHAPE_CUBOID = 0, CPS_SHAPE_ELLIPSOID = 1, CPS_SHAPE_CYLINDER = 2, CPS_SHAPE_MULTI = 3 };
+typedef struct cps_shape {
+    int32_t type;
+    int32_t material_index;
+    double theta, phi, psi;
+    double x0, y0, z0;
+    double a, b, c;
+} cps_shape;
+
+CPS_API const char *cps_last_error(void);
+CPS_API const char *cps_version(void);
+CPS_API double cps_courant_dt(double dx, double dy, double dz);
+
+/* ---- grid lifetime ---- */
+CPS_API cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out);
+CPS_API cps_status cps_grid_destroy(cps_grid *g);
+CPS_API cps_status cps_grid_info(const cps_grid *g, cps_grid_desc *out);
+/* device bytes the grid holds now */
+CPS_API cps_status cps_grid_bytes(const cps_grid *g, int64_t *bytes);
+/* CUDA stream (cudaStream_t) all work of the grid is enqueued on; NULL = the
+ * grid's own stream */
+CPS_API cps_status cps_grid_set_stream(cps_grid *g, void *stream);
+CPS_API cps_status cps_grid_get_stream(const cps_grid *g, void **stream);
+CPS_API cps_status cps_synchronize(cps_grid *g);
+
+/* ---- geometry and media ---- */
+CPS_API cps_status cps_grid_set_media(cps_grid *g, int32_t n, const double *epsR, const double *muR,
+                                      const double *sig, const double *sigM);
+CPS_API cps_status cps_grid_upload_ids(cps_grid *g, const uint8_t *ids);
+CPS_API cps_status cps_grid_download_ids(const cps_grid *g, uint8_t *ids);
+/* Rasterise shapes into a host ID grid exactly as Structure::generate_mesh does
+ * (ids must hold (nx+1)(ny+1)(nz+1) bytes, [i][j][k]; it is overwritten with 0
+ * first unless keep != 0). */
+CPS_API cps_status cps_mesh_rasterize(int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                                      int32_t nshapes, const cps_shape *shapes, uint8_t *ids, int32_t keep);
+
+/* ---- physics modules (call after media and IDs are set) ---- */
+CPS_API cps_status cps_pml_init(cps_grid *g, const cps_pml_params *p);
+CPS_API cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p);
+CPS_API cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p);
+CPS_API cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p);
+/* replace the incident tables Einc/Hinc (n = Nt + 1 values each) */
+CPS_API cps_status cps_tfsf_set_tables(cps_grid *g, int32_t n, const double *einc, const double *hinc);
+CPS_API cps_status cps_tfsf_get_tables(const cps_grid *g, int32_t n, double *einc, double *hinc);
+/* additive source: field comp at (i,j,k) += wave[n] at step n (0 <= n < nwave) */
+CPS_API cps_status cps_source_add(cps_grid *g, int32_t comp, int32_t i, int32_t j, int32_t k,
+                                  const double *wave, int32_t nwave);
+
+/* ---- ports ---- */
+/* point sets of the reference constructors; call with ijk = NULL to get the
+ * count, then with room for 3*count int32 */
+CPS_API cps_status cps_port_points_plain(int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                                         char normal, double position, double w1, double w2, double h1,
+                                         double h2, int32_t *count, int32_t *ijk);
+CPS_API cps_status cps_port_points_spherical(int32_t nx, int32_t ny, int32_t nz, double dx, double dy,
+                                             double dz, double r, double xc, double yc, double zc,
+                                             double theta1_deg, double theta2_deg, double phi1_deg,
+                                             double phi2_deg, int32_t *count, int32_t *ijk);
+CPS_API cps_status cps_port_add(cps_grid *g, int32_t npoints, const int32_t *ijk, int32_t *port_id);
+/* running DFT of the samples at nfreq frequencies (Hz) for the components in
+ * comp_mask (bit c = component c); FP64 accumulators on the device */
+CPS_API cps_status cps_port_set_dft(cps_grid *g, int32_t port_id, int32_t nfreq, const double *freq_hz,
+                                    uint32_t comp_mask);
+/* last sample, [npoints][6] */
+CPS_API cps_status cps_port_read(cps_grid *g, int32_t port_id, double *out);
+/* DFT accumulators, [ncomp][nfreq][2][npoints]: for each component (ascending)
+ * and frequency a plane of real parts then a plane of imaginary parts */
+CPS_API cps_status cps_port_dft_read(cps_grid *g, int32_t port_id, double *out);
+/* net Poynting flux 0.5*Re(sum_p (E x conj H) . n dA) per frequency through a
+ * planar port whose DFT holds the four tangential components; normal = 'x','y','z' */
+CPS_API cps_status cps_port_flux(cps_grid *g, int32_t port_id, char normal, double *out);
+
+/* ---- time stepping ---- */
+/* step index n used by TF/SF and sources; main.cpp's loop starts at 1 */
+CPS_API cps_status cps_grid_set_step(cps_grid *g, int64_t n);
+CPS_API cps_status cps_grid_get_step(const cps_grid *g, int64_t *n);
+/* advance nsteps steps, each in the order of main.cpp:267-344: H bulk, TF/SF H,
+ * CPML H, E bulk, Drude-Lorentz, gain (P, E, N), TF/SF E, sources, CPML E,
+ * port sampling.  Asynchronous on the grid's stream. */
+CPS_API cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path);
+
+/* ---- single reference routines (one launch each, enqueued on the grid's stream) ---- */
+CPS_API cps_status cps_op_h_bulk(cps_grid *g);
+CPS_API cps_status cps_op_e_bulk(cps_grid *g);
+CPS_API cps_status cps_op_h_pml(cps_grid *g);
+CPS_API cps_status cps_op_e_pml(cps_grid *g);
+CPS_API cps_status cps_op_dl(cps_grid *g);
+CPS_API cps_status cps_op_gain_polarization(cps_grid *g);
+CPS_API cps_status cps_op_gain_efield(cps_grid *g);
+CPS_API cps_status cps_op_gain_populations(cps_grid *g);
+CPS_API cps_status cps_op_tfsf_h(cps_grid *g, int32_t n, uint32_t face_mask);
+CPS_API cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask);
+CPS_API cps_status cps_op_sources(cps_grid *g, int32_t n);
+CPS_API cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n);
+
+/* ---- field access ---- */
+CPS_API cps_status cps_field_download(cps_grid *g, int32_t comp, double *out);
+CPS_API cps_status cps_field_upload(cps_grid *g, int32_t comp, const double *in);
+CPS_API cps_status cps_field_download_f32(cps_grid *g, int32_t comp, float *out);
+/* reset fields, auxiliary state, port samples and DFT accumulators to zero
+ * (initial populations for gain) and the step index to n0 */
+CPS_API cps_status cps_grid_reset(cps_grid *g, int64_t n0);
+/* count of non-finite field values (device reduction) */
+CPS_API cps_status cps_grid_check_finite(cps_grid *g, int64_t *nonfinite);
+/* FP64 gain populations, [ncells][4] N0..N3, cells in (i,j,k) order */
+CPS_API cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *ncells);
+/* number of kernel launches this grid has enqueued since creation */
+CPS_API cps_status cps_grid_launch_count(const cps_grid *g, int64_t *launches);
+/* fold the port samples still held in the rings into the DFT accumulators
+ * (the read-out calls do this themselves) */
+CPS_API cps_status cps_ports_flush(cps_grid *g);
+/* sweep timing: with stride > 0, cps_step records CUDA events on the grid's
+ * stream around the H and E sweeps of every stride-th step (at most 4096
+ * samples); cps_grid_timing synchronises and returns their mean durations in
+ * milliseconds.  stride 0 turns it off and clears the samples. */
+CPS_API cps_status cps_grid_set_timing(cps_grid *g, int32_t stride);
+CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sweep_ms, int64_t *samples);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

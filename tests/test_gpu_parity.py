@@ -1,0 +1,100 @@
+"""CUDA engine against the FP64 oracle, through the C ABI.
+
+Bars (per field component, relative L2 after N steps):
+  FP64 grids, plain and fused paths: <= 1e-10
+  FP32 grids, fused path:           <= 1e-4
+Port samples and port DFT accumulators use the same bars."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from cpsfdtd_b200 import decks
+import golden.golden_cases as gc
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 1e-4
+NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def _setup(dk, oracle_mod):
+    import cpsfdtd_b200 as cps
+    ids = dk.ids if dk.ids is not None else cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    pts = [cps.port_points(dk, p) for p in dk.ports]
+    o = oracle_mod.Oracle.from_deck(dk, ids, pts)
+    o.step(dk.nsteps)
+    return ids, pts, o
+
+
+CASES = {"c1": lambda: decks.config1(n=32, steps=120),
+         "c2": lambda: decks.config2(n=48, steps=100, nfreq=8),
+         "c2_cw": gc.c2_cw,
+         "c3": lambda: decks.config3(n=40, steps=100, nfreq=4),
+         "shapes": gc.shapes_pec}
+
+
+@pytest.fixture(scope="module")
+def oracle_runs(oracle_mod):
+    return {k: (f(), ) + _setup(f(), oracle_mod) for k, f in CASES.items()}
+
+
+def _check(g, dk, pts, o, tol, tag):
+    for c in range(6):
+        want = o.field(c)
+        if np.linalg.norm(want) == 0:
+            assert np.abs(g.field(c)).max() == 0, f"{tag} {NAMES[c]} should stay zero"
+            continue
+        err = rel_l2(g.field(c), want)
+        assert err <= tol, f"{tag} {NAMES[c]} rel L2 {err:.3e} > {tol:.0e}"
+    for n, p in enumerate(dk.ports):
+        err = rel_l2(g.port_last(n), o.port_last(n))
+        assert err <= tol, f"{tag} port {n} samples rel L2 {err:.3e}"
+        if p.dft_freqs is not None:
+            ncomp = bin(p.dft_mask).count("1")
+            want = o.port_dft(n, ncomp, len(p.dft_freqs))
+            err = rel_l2(g.port_dft(n), want)
+            assert err <= tol, f"{tag} port {n} DFT rel L2 {err:.3e}"
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("path", [0, 1], ids=["plain", "fused"])
+def test_fp64_matches_oracle(case, path, oracle_runs):
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs[case]
+    g = cps.Grid.from_deck(dk, cps.FP64, ids=ids, port_points_list=pts)
+    g.step(dk.nsteps, path)
+    _check(g, dk, pts, o, FP64_TOL, f"{case}/fp64/{'plain' if path == 0 else 'fused'}")
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fp32_fused_matches_oracle(case, oracle_runs):
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs[case]
+    g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts)
+    g.step(dk.nsteps, cps.FUSED)
+    _check(g, dk, pts, o, FP32_TOL, f"{case}/fp32/fused")
+
+
+def test_fp64_plain_is_bit_exact_on_dielectric_cpml(oracle_runs):
+    """Without FMA contraction the plain FP64 kernels follow the reference's
+    roundings: C1 (dielectric + CPML + source + port) agrees bit for bit."""
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs["c1"]
+    g = cps.Grid.from_deck(dk, cps.FP64, ids=ids, port_points_list=pts)
+    g.step(dk.nsteps, cps.PLAIN)
+    for c in range(6):
+        assert np.array_equal(g.field(c), o.field(c)), NAMES[c]
+
+
+def test_gain_populations_match_oracle(oracle_mod, oracle_runs):
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs["c3"]
+    want = o.populations()
+    for prec, tol in ((cps.FP64, 1e-12), (cps.FP32, 1e-6)):
+        g = cps.Grid.from_deck(dk, prec, ids=ids, port_points_list=pts)
+        g.step(dk.nsteps, cps.FUSED)
+        got = g.populations()
+        assert got.shape == want.shape
+        assert np.abs(got - want).max() <= tol
+        assert np.abs(got.sum(axis=1) - 2.0).max() < 1e-12  # conservation, FourLevelLaser.cpp:324
