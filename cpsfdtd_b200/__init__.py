@@ -121,6 +121,8 @@ def lib():
             "cps_gain_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_grid_launch_count": ([P, C.POINTER(I64)], I32),
             "cps_ports_flush": ([P], I32), "cps_grid_set_timing": ([P, I32], I32),
+            "cps_grid_set_tile": ([P, I32, I32], I32), "cps_grid_get_tile": ([P, ip, ip], I32),
+            "cps_grid_set_sweep": ([P, I32], I32),
             "cps_grid_timing": ([P, C.POINTER(D), C.POINTER(D), C.POINTER(I64)], I32),
         }
         for name, (args, res) in sigs.items():
@@ -370,6 +372,18 @@ class Grid:
         h, e, n = C.c_double(), C.c_double(), C.c_int64()
         _check(self.L.cps_grid_timing(self.h, C.byref(h), C.byref(e), C.byref(n)))
         return h.value, e.value, n.value
+
+    def set_tile(self, rows, planes):
+        _check(self.L.cps_grid_set_tile(self.h, rows, planes))
+
+    def set_sweep(self, mode):
+        """0: TMA-fed sweeps (default), 1: register sweeps."""
+        _check(self.L.cps_grid_set_sweep(self.h, mode))
+
+    def get_tile(self):
+        r, p = C.c_int32(), C.c_int32()
+        _check(self.L.cps_grid_get_tile(self.h, C.byref(r), C.byref(p)))
+        return r.value, p.value
 
     def stream(self):
         p = C.c_void_p()

@@ -30,6 +30,7 @@ SOURCES = {
     "host_setup.cpp": ["-x", "cu"],
     "kernels_plain.cu": ["--fmad=false"],
     "kernels_fused.cu": [],
+    "kernels_tma.cu": [],
     "kernels_ports.cu": [],
 }
 

@@ -133,9 +133,14 @@ struct cps_grid {
     // misc
     int64_t step = 1;
     int64_t launches = 0;
-    FusedShape shape{8, 32};
+    FusedShape shape{4, 8};
     double *d_conv = nullptr;
     unsigned long long *d_counter = nullptr;
+    // TMA tensor maps of the fused sweeps (built for tile rows tma_by)
+    TmaMaps tma{};
+    int tma_by = 0;
+    int sweep_mode = 0;  // 0: TMA-fed sweeps, 1: register sweeps
+    int *d_err = nullptr;  // set by a device wait that gave up
     // sweep timing samples: events (start, after H sweep, after E sweep)
     int timing_stride = 0;
     std::vector<cudaEvent_t> ev;
@@ -439,21 +444,41 @@ void op_sources(cps_grid *g, int n)
     g->launches++;
 }
 
+// Sample ports into their rings (Update_Fields_on_Port), all ports of the
+// list in one launch; a full ring is first folded into the DFT accumulators.
+template <typename T>
+cps_status op_ports(cps_grid *g, PortState *const *ports, int nports, int64_t n)
+{
+    for (int b0 = 0; b0 < nports; b0 += kMaxGather) {
+        GatherBatch B;
+        memset(&B, 0, sizeof(B));
+        for (int q = b0; q < nports && q < b0 + kMaxGather; ++q) {
+            PortState &P = *ports[q];
+            if (P.fill == P.slots) {
+                cps_status s = flush_dft(g, P);
+                if (s) return s;
+            }
+            if (P.fill == 0) P.ring_n0 = n;
+            GatherDesc &D = B.p[B.n++];
+            D.idx = P.d_idx;
+            D.slot = (T *)P.d_ring + (int64_t)P.fill * 6 * P.npts;
+            D.npts = P.npts;
+            B.max_npts = std::max(B.max_npts, P.npts);
+            P.last_slot = P.fill;
+            P.fill++;
+            if (P.nfreq == 0) P.fill = 0;  // no DFT: the ring holds the last sample only
+        }
+        launch_port_gather<T>(field_view<T>(g), B, g->stream);
+        g->launches++;
+    }
+    return CPS_OK;
+}
+
 template <typename T>
 cps_status op_port(cps_grid *g, PortState &P, int64_t n)
 {
-    if (P.fill == P.slots) {
-        cps_status s = flush_dft(g, P);
-        if (s) return s;
-    }
-    if (P.fill == 0) P.ring_n0 = n;
-    T *slot = (T *)P.d_ring + (int64_t)P.fill * 6 * P.npts;
-    launch_port_gather<T>(field_view<T>(g), P.d_idx, P.npts, slot, g->stream);
-    g->launches++;
-    P.last_slot = P.fill;
-    P.fill++;
-    if (P.nfreq == 0) P.fill = 0;  // no DFT: the ring holds the last sample only
-    return CPS_OK;
+    PortState *one = &P;
+    return op_ports<T>(g, &one, 1, n);
 }
 
 template <typename T>
@@ -485,11 +510,73 @@ cps_status flush_dft(cps_grid *g, PortState &P)
     return g->fp32 ? flush_dft_T<float>(g, P) : flush_dft_T<double>(g, P);
 }
 
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn()
+{
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)p;
+    });
+    return fn;
+}
+
+// tensor maps of the six fields and the IDs for tiles of `by` rows
+cps_status ensure_tma(cps_grid *g)
+{
+    const int by = g->shape.by;
+    if (g->tma_by == by) return CPS_OK;
+    EncodeTiled enc = encode_fn();
+    REQUIRE(enc, CPS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const Dims &d = g->d;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.px, (cuuint64_t)(d.ny + 1), (cuuint64_t)(d.nz + 1)};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = g->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t st[2] = {(cuuint64_t)d.px * g->esz, (cuuint64_t)d.pxy * g->esz};
+    const cuuint32_t halo[3] = {36, (cuuint32_t)by + 1, 1}, own[3] = {32, (cuuint32_t)by, 1};
+    for (int c = 0; c < 6; ++c) {
+        CUresult r1 = enc(&g->tma.halo[c], dt, 3, g->F[c], dims, st, halo, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r2 = enc(&g->tma.own[c], dt, 3, g->F[c], dims, st, own, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        REQUIRE(r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for a field");
+    }
+    const cuuint64_t sid[2] = {(cuuint64_t)d.px, (cuuint64_t)d.pxy};
+    CUresult r = enc(&g->tma.id, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, g->d_id, dims, sid, own, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    REQUIRE(r == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for the IDs");
+    g->tma_by = by;
+    return CPS_OK;
+}
+
+cps_status check_device_error(cps_grid *g)
+{
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, g->d_err, sizeof(int), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    REQUIRE(e == 0, CPS_E_TIMEOUT, "a device-side wait of a sweep gave up (TMA data did not arrive)");
+    return CPS_OK;
+}
+
 template <typename T>
 cps_status step_T(cps_grid *g, int nsteps, int path)
 {
     cps_status s = ensure_sources(g);
     if (s) return s;
+    // TMA boxes are 36 x (rows+1): grids narrower than that use the register sweeps
+    const bool use_tma = path == CPS_PATH_FUSED && g->sweep_mode == 0 && (g->shape.by == 4 || g->shape.by == 8) &&
+                         g->d.px >= 64 && g->d.ny + 1 >= g->shape.by + 1;
+    if (use_tma && (s = ensure_tma(g))) return s;
     const FieldView<T> f = field_view<T>(g);
     const PmlView<T> p = pml_view<T>(g);
     const DlView<T> D = dl_view<T>(g);
@@ -515,11 +602,13 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             const bool timed = g->timing_stride > 0 && n % g->timing_stride == 0 &&
                                g->ev_used + 4 <= (int)g->ev.size();
             if (timed) cudaEventRecord(g->ev[g->ev_used], g->stream);
-            launch_h_fused<T>(f, p, g->shape, g->stream);
+            if (use_tma) launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
+            else launch_h_fused<T>(f, p, g->shape, g->stream);
             if (timed) cudaEventRecord(g->ev[g->ev_used + 1], g->stream);
             op_inject<T>(g, 1, (double)n, CPS_FACE_ALL);
             if (timed) cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
-            launch_e_fused<T>(f, p, D, G, g->shape, g->stream);
+            if (use_tma) launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream);
+            else launch_e_fused<T>(f, p, D, G, g->shape, g->stream);
             if (timed) {
                 cudaEventRecord(g->ev[g->ev_used + 3], g->stream);
                 g->ev_used += 4;
@@ -528,8 +617,10 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             op_sources<T>(g, (int)n);
             g->launches += 2;
         }
-        for (PortState &P : g->ports) {
-            s = op_port<T>(g, P, n);
+        if (!g->ports.empty()) {
+            std::vector<PortState *> all;
+            for (PortState &P : g->ports) all.push_back(&P);
+            s = op_ports<T>(g, all.data(), (int)all.size(), n);
             if (s) return s;
         }
         g->step++;
@@ -580,6 +671,7 @@ extern "C" cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out)
     if (!s) s = dalloc(g, (void **)&g->d_id, (size_t)g->elems);
     if (!s) s = dalloc(g, &g->d_media, 4 * 256 * g->esz);
     if (!s) s = dalloc(g, (void **)&g->d_counter, sizeof(unsigned long long));
+    if (!s) s = dalloc(g, (void **)&g->d_err, sizeof(int));
     if (s) { cps_grid_destroy(g); return s; }
     g->ids_dev.assign((size_t)g->elems, 0);
     // stretched coordinates start at 1/delta (Structure.cpp:425-445)
@@ -645,7 +737,7 @@ extern "C" cps_status cps_synchronize(cps_grid *g)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
     CK(cudaStreamSynchronize(g->stream));
-    return CPS_OK;
+    return check_device_error(g);
 }
 
 // ================================================================ geometry
@@ -767,7 +859,7 @@ extern "C" cps_status cps_pml_init(cps_grid *g, const cps_pml_params *pp)
     for (int f = 0; f < 6; ++f) {
         const int np = pp->npml[f];
         size_t n;
-        if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * (np + 1);
+        if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * psi_xw(np);
         else if (f < 4) n = (size_t)(d.nz + 1) * (np + 1) * d.px;
         else n = (size_t)(np + 1) * (d.ny + 1) * d.px;
         for (int q = 0; q < 4; ++q)
@@ -990,6 +1082,9 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
         }
         std::vector<InjTarget> tg;
         std::vector<InjContrib> ct;
+        // targets in device order, so neighbouring threads touch neighbouring cells;
+        // each target keeps its contributions in the reference's face order
+        std::sort(keys.begin(), keys.end());
         for (int64_t key : keys) {
             const std::vector<InjContrib> &v = per[key];
             InjTarget t;
@@ -1349,7 +1444,7 @@ extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
         for (int f = 0; f < 6; ++f) {
             const int np = g->pml.npml[f];
             size_t n;
-            if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * (np + 1);
+            if (f < 2) n = (size_t)(d.nz + 1) * (d.ny + 1) * psi_xw(np);
             else if (f < 4) n = (size_t)(d.nz + 1) * (np + 1) * d.px;
             else n = (size_t)(np + 1) * (d.ny + 1) * d.px;
             for (int q = 0; q < 4; ++q) CK(cudaMemsetAsync(g->d_q[f][q], 0, n * g->esz, g->stream));
@@ -1478,5 +1573,31 @@ extern "C" cps_status cps_grid_timing(cps_grid *g, double *h_ms, double *e_ms, i
     *h_ms = n ? h / n : 0.0;
     *e_ms = n ? e / n : 0.0;
     *samples = n;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_set_tile(cps_grid *g, int32_t rows, int32_t planes)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    REQUIRE((rows == 4 || rows == 8 || rows == 16) && planes >= 1, CPS_E_INVALID,
+            "cps_grid_set_tile: rows must be 4, 8 or 16 and planes >= 1");
+    g->shape.by = rows;
+    g->shape.kc = planes;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *planes)
+{
+    REQUIRE(g && rows && planes, CPS_E_INVALID, "NULL argument");
+    *rows = g->shape.by;
+    *planes = g->shape.kc;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_set_sweep(cps_grid *g, int32_t mode)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    REQUIRE(mode == 0 || mode == 1, CPS_E_INVALID, "cps_grid_set_sweep: 0 (TMA-fed) or 1 (register)");
+    g->sweep_mode = mode;
     return CPS_OK;
 }

@@ -32,6 +32,10 @@ constexpr double kHPlanck = 6.62607004081E-34;
 constexpr double kMu0 = 1.2566370614E-6;
 constexpr double kEps0 = 8.8541878176E-12;
 
+// row width of an x-slab psi array ([k][j][s], s = 0..np): np+1 rounded up to
+// 32 words so every row starts on a 128-byte line
+__host__ __device__ inline int psi_xw(int np) { return (np + 32) / 32 * 32; }
+
 struct Dims {
     int nx, ny, nz;   // cells
     int px;           // x pitch in elements
@@ -159,10 +163,32 @@ template <typename T>
 void launch_e_fused(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &d,
                     const GainView<T> &g, FusedShape sh, cudaStream_t s);
 
-// Ports (kernels_ports.cu)
+// TMA-fed fused sweeps (kernels_tma.cu); rows per block 4 or 8
+}  // namespace cps
+#include "tma.cuh"
+namespace cps {
 template <typename T>
-void launch_port_gather(const FieldView<T> &f, const int64_t *idx, int npts, T *ring_slot,
-                        cudaStream_t s);
+void launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
+                  cudaStream_t s);
+template <typename T>
+void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+                  const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s);
+
+// Ports (kernels_ports.cu)
+constexpr int kMaxGather = 16;
+struct GatherDesc {
+    const int64_t *idx;
+    void *slot;  // ring slot [6][npts] of T
+    int npts;
+    int pad;
+};
+struct GatherBatch {
+    GatherDesc p[kMaxGather];
+    int n;
+    int max_npts;
+};
+template <typename T>
+void launch_port_gather(const FieldView<T> &f, const GatherBatch &b, cudaStream_t s);
 template <typename T>
 void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, double dt,
                      const double *omega, int nfreq, const int32_t *comps, int ncomp,

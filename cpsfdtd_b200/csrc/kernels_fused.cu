@@ -2,9 +2,12 @@
 //
 // Each block covers a 32 x BY patch of (i, j) columns and marches KC planes
 // in k.  A thread keeps the k-neighbour of its own column in registers (E at
-// k+1 for H, H at k-1 for E), so every field word crosses HBM once per sweep;
-// the x/y neighbours come from the L1 lines the neighbouring threads of the
-// same block load.  Per cell the sweep applies, in the reference order:
+// k+1 for H, H at k-1 for E), takes its x-neighbour from the adjacent lane by
+// a warp shuffle, and reads the y-neighbour through L1, so every field word
+// crosses HBM once per sweep.  All loads of plane k+1 are issued (read-only,
+// non-coherent path) before plane k is computed and stored, which keeps two
+// planes of loads in flight per thread.
+// Per cell the sweep applies, in the reference order:
 //   H: bulk (BasicFDTD.cpp:67-84) then CPML psi corrections (CPML.cpp:609-689)
 //   E: bulk (BasicFDTD.cpp:25-47), Drude-Lorentz (ID 2), four-level gain
 //      (P, E, N), then CPML (CPML.cpp:529-607).
@@ -26,45 +29,84 @@ __device__ __forceinline__ unsigned lanemask_lt()
     return m;
 }
 
+template <typename T>
+__device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
+
+// values of one plane that the H sweep of a column needs
+template <typename T>
+struct HPlane {
+    T exk, eyk;        // E at k+1 of the own column
+    T ez, ezj, exj;    // Ez own, Ez(j+1), Ex(j+1)
+    T ezi, eyi;        // Ez(i+1), Ey(i+1): only lane 31 loads them
+    T hx, hy, hz;
+    int id;
+};
+
+template <typename T>
+__device__ __forceinline__ void h_load(HPlane<T> &q, const FieldView<T> &f, int64_t g, bool last_lane, bool ok)
+{
+    const Dims &d = f.d;
+    q.exk = ldg(&f.Ex[g + d.pxy]);
+    q.eyk = ldg(&f.Ey[g + d.pxy]);
+    q.ez = ldg(&f.Ez[g]);
+    q.ezj = ldg(&f.Ez[g + d.px]);
+    q.exj = ldg(&f.Ex[g + d.px]);
+    q.ezi = (last_lane && ok) ? ldg(&f.Ez[g + 1]) : T(0);
+    q.eyi = (last_lane && ok) ? ldg(&f.Ey[g + 1]) : T(0);
+    q.hx = ldg(&f.Hx[g]);
+    q.hy = ldg(&f.Hy[g]);
+    q.hz = ldg(&f.Hz[g]);
+    q.id = ldg(&f.id[g]);
+}
+
 template <typename T, int BY, bool PML>
-__global__ void __launch_bounds__(32 * BY) k_h_fused(FieldView<T> f, PmlView<T> p, int kc)
+__global__ void __launch_bounds__(32 * BY, (768 / (32 * BY)) > 0 ? 768 / (32 * BY) : 1)
+k_h_fused(FieldView<T> f, PmlView<T> p, int kc)
 {
     const Dims d = f.d;
-    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+    const int lane = threadIdx.x;
+    const int i = blockIdx.x * 32 + lane, j = blockIdx.y * BY + threadIdx.y;
     const int k0 = blockIdx.z * kc, k1 = min(k0 + kc, d.nz);
-    if (i >= d.nx || j >= d.ny) return;
+    // a warp is one row; rows outside [0, ny-1] leave whole, lanes past nx-1
+    // load their (padded, in-bounds) cell for the shuffles but store nothing
+    if (j >= d.ny || k0 >= k1) return;
+    const bool act = i < d.nx;
     const StretchView<T> &s = f.s;
-    const T cHyz = s.cHyz[i], cHzy = s.cHzy[i], cHxz = s.cHxz[j], cHzx = s.cHzx[j];
-    // CPML slabs this column belongs to (x and y are fixed along the march)
+    const int ic = act ? i : d.nx - 1;
+    const T cHyz = s.cHyz[ic], cHzy = s.cHzy[ic], cHxz = s.cHxz[j], cHzx = s.cHzx[j];
     int fx = -1, sxl = 0, fy = -1, syl = 0;
     T bx = 0, cx = 0, by = 0, cy = 0;
     if (PML) {
         if (i < p.np[kFX1]) { fx = kFX1; sxl = i; }
-        else if (i >= d.nx - p.np[kFX2]) { fx = kFX2; sxl = i - (d.nx - p.np[kFX2]); }
+        else if (act && i >= d.nx - p.np[kFX2]) { fx = kFX2; sxl = i - (d.nx - p.np[kFX2]); }
         if (j < p.np[kFY1]) { fy = kFY1; syl = j; }
         else if (j >= d.ny - p.np[kFY2]) { fy = kFY2; syl = j - (d.ny - p.np[kFY2]); }
         if (fx >= 0) { bx = p.bH[fx][sxl]; cx = p.cH[fx][sxl]; }
         if (fy >= 0) { by = p.bH[fy][syl]; cy = p.cH[fy][syl]; }
     }
+    const bool last = lane == 31;
     int64_t g = d.idx(i, j, k0);
-    T ex = f.Ex[g], ey = f.Ey[g];
+    T ex = ldg(&f.Ex[g]), ey = ldg(&f.Ey[g]);
+    HPlane<T> cur, nxt;
+    h_load(cur, f, g, last, act);
     for (int k = k0; k < k1; ++k, g += d.pxy) {
-        const T exk = f.Ex[g + d.pxy], eyk = f.Ey[g + d.pxy];
-        const T ez = f.Ez[g];
-        const T dEz_i = ld(&f.Ez[g + 1]) - ez, dEz_j = ld(&f.Ez[g + d.px]) - ez;
-        const T dEx_j = ld(&f.Ex[g + d.px]) - ex, dEy_i = ld(&f.Ey[g + 1]) - ey;
-        const T dEx_k = exk - ex, dEy_k = eyk - ey;
-        const int id = f.id[g];
-        const T aH = ld(&f.aH[id]), bH = ld(&f.bH[id]);
-        T hx = f.Hx[g], hy = f.Hy[g], hz = f.Hz[g];
-        hx = aH * hx - bH * dEz_j * cHxz + bH * dEy_k * s.cHxy[k];
-        hy = aH * hy - bH * dEx_k * s.cHyx[k] + bH * dEz_i * cHyz;
-        hz = aH * hz + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
-        if (PML) {
+        if (k + 1 < k1) h_load(nxt, f, g + d.pxy, last, act);
+        // x-neighbours from lane + 1
+        T ezi = __shfl_down_sync(0xffffffffu, cur.ez, 1);
+        T eyi = __shfl_down_sync(0xffffffffu, ey, 1);
+        if (last) { ezi = cur.ezi; eyi = cur.eyi; }
+        const T dEz_i = ezi - cur.ez, dEz_j = cur.ezj - cur.ez;
+        const T dEx_j = cur.exj - ex, dEy_i = eyi - ey;
+        const T dEx_k = cur.exk - ex, dEy_k = cur.eyk - ey;
+        const T aH = ldg(&f.aH[cur.id]), bH = ldg(&f.bH[cur.id]);
+        T hx = aH * cur.hx - bH * dEz_j * cHxz + bH * dEy_k * ldg(&s.cHxy[k]);
+        T hy = aH * cur.hy - bH * dEx_k * ldg(&s.cHyx[k]) + bH * dEz_i * cHyz;
+        T hz = aH * cur.hz + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
+        if (PML && act) {
             const T ch = p.cpmlH;
             if (fx >= 0) {
                 const int np = p.np[fx];
-                const int64_t q = ((int64_t)k * (d.ny + 1) + j) * (np + 1) + sxl;
+                const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + sxl;
                 T *q0 = p.qh[fx][0], *q1 = p.qh[fx][1];
                 const T a0 = bx * q0[q] + cx * dEz_i, a1 = bx * q1[q] + cx * dEy_i;
                 q0[q] = a0; q1[q] = a1;
@@ -93,20 +135,49 @@ __global__ void __launch_bounds__(32 * BY) k_h_fused(FieldView<T> f, PmlView<T> 
                 hy = hy + a1 * ch;
             }
         }
-        f.Hx[g] = hx; f.Hy[g] = hy; f.Hz[g] = hz;
-        ex = exk; ey = eyk;
+        if (act) { f.Hx[g] = hx; f.Hy[g] = hy; f.Hz[g] = hz; }
+        ex = cur.exk; ey = cur.eyk;
+        cur = nxt;
     }
 }
 
+// values of one plane that the E sweep of a column needs
+template <typename T>
+struct EPlane {
+    T hx, hy, hz;      // own H
+    T hzj, hxj;        // Hz(j-1), Hx(j-1)
+    T hzi, hyi;        // Hz(i-1), Hy(i-1): only lane 0 loads them
+    T ex, ey, ez;
+    int id;
+};
+
+template <typename T>
+__device__ __forceinline__ void e_load(EPlane<T> &q, const FieldView<T> &f, int64_t g, bool first_lane, bool has_left)
+{
+    const Dims &d = f.d;
+    q.hx = ldg(&f.Hx[g]);
+    q.hy = ldg(&f.Hy[g]);
+    q.hz = ldg(&f.Hz[g]);
+    q.hzj = ldg(&f.Hz[g - d.px]);
+    q.hxj = ldg(&f.Hx[g - d.px]);
+    q.hzi = (first_lane && has_left) ? ldg(&f.Hz[g - 1]) : T(0);
+    q.hyi = (first_lane && has_left) ? ldg(&f.Hy[g - 1]) : T(0);
+    q.ex = ldg(&f.Ex[g]);
+    q.ey = ldg(&f.Ey[g]);
+    q.ez = ldg(&f.Ez[g]);
+    q.id = ldg(&f.id[g]);
+}
+
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
-__global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> p, DlView<T> D,
-                                                     GainView<T> G, int kc)
+__global__ void __launch_bounds__(32 * BY, (768 / (32 * BY)) > 0 ? 768 / (32 * BY) : 1)
+k_e_fused(FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc)
 {
     const Dims d = f.d;
-    const int i = blockIdx.x * 32 + threadIdx.x, j = blockIdx.y * BY + threadIdx.y;
+    const int lane = threadIdx.x;
+    const int i = blockIdx.x * 32 + lane, j = blockIdx.y * BY + threadIdx.y;
     const int k0 = max(1, blockIdx.z * kc), k1 = min(blockIdx.z * kc + kc, d.nz);
     // a warp is one row j; rows outside [1, ny-1] leave whole, lanes outside
-    // [1, nx-1] stay for the ballots but touch no memory
+    // [1, nx-1] load their (in-bounds) cell for the shuffles but store nothing
     if (j < 1 || j >= d.ny || k0 >= k1) return;
     const bool act = i >= 1 && i < d.nx;
     const int ic = act ? i : 1;
@@ -115,38 +186,36 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
     int fx = -1, sxl = 0, fy = -1, syl = 0;
     T bx = 0, cx = 0, by = 0, cy = 0;
     if (PML) {
-        if (ic <= p.np[kFX1]) { fx = kFX1; sxl = ic; }
-        else if (ic >= d.nx - p.np[kFX2]) { fx = kFX2; sxl = ic - (d.nx - p.np[kFX2]); }
+        if (act && i <= p.np[kFX1]) { fx = kFX1; sxl = i; }
+        else if (act && i >= d.nx - p.np[kFX2]) { fx = kFX2; sxl = i - (d.nx - p.np[kFX2]); }
         if (j <= p.np[kFY1]) { fy = kFY1; syl = j; }
         else if (j >= d.ny - p.np[kFY2]) { fy = kFY2; syl = j - (d.ny - p.np[kFY2]); }
         if (fx >= 0) { bx = p.bE[fx][sxl]; cx = p.cE[fx][sxl]; }
         if (fy >= 0) { by = p.bE[fy][syl]; cy = p.cE[fy][syl]; }
     }
     const int nseg = d.px >> 5;
-    int64_t g = d.idx(ic, j, k0);
-    T hxm = act ? f.Hx[g - d.pxy] : T(0), hym = act ? f.Hy[g - d.pxy] : T(0);
+    const bool first = lane == 0, has_left = i > 0;
+    int64_t g = d.idx(i, j, k0);
+    T hxm = ldg(&f.Hx[g - d.pxy]), hym = ldg(&f.Hy[g - d.pxy]);
+    EPlane<T> cur, nxt;
+    e_load(cur, f, g, first, has_left);
     for (int k = k0; k < k1; ++k, g += d.pxy) {
-        T hx = 0, hy = 0, hz = 0, ex = 0, ey = 0, ez = 0;
-        T dHz_j = 0, dHy_k = 0, dHx_k = 0, dHz_i = 0, dHy_i = 0, dHx_j = 0;
-        int id = 0;
-        if (act) {
-            hx = f.Hx[g]; hy = f.Hy[g]; hz = f.Hz[g];
-            dHz_j = hz - ld(&f.Hz[g - d.px]);
-            dHz_i = hz - ld(&f.Hz[g - 1]);
-            dHy_i = hy - ld(&f.Hy[g - 1]);
-            dHx_j = hx - ld(&f.Hx[g - d.px]);
-            dHy_k = hy - hym;
-            dHx_k = hx - hxm;
-            ex = f.Ex[g]; ey = f.Ey[g]; ez = f.Ez[g];
-            id = f.id[g];
-            if (id == CPS_ID_PEC) {
-                ex = T(0); ey = T(0); ez = T(0);
-            } else if (id != CPS_ID_DISPERSIVE) {
-                const T aE = ld(&f.aE[id]), bE = ld(&f.bE[id]);
-                ex = aE * ex + bE * dHz_j * cExz - bE * dHy_k * s.cExy[k];
-                ey = aE * ey + bE * dHx_k * s.cEyx[k] - bE * dHz_i * cEyz;
-                ez = aE * ez + bE * dHy_i * cEzy - bE * dHx_j * cEzx;
-            }
+        if (k + 1 < k1) e_load(nxt, f, g + d.pxy, first, has_left);
+        T hzi = __shfl_up_sync(0xffffffffu, cur.hz, 1);
+        T hyi = __shfl_up_sync(0xffffffffu, cur.hy, 1);
+        if (first) { hzi = cur.hzi; hyi = cur.hyi; }
+        const T dHz_j = cur.hz - cur.hzj, dHz_i = cur.hz - hzi, dHy_i = cur.hy - hyi;
+        const T dHx_j = cur.hx - cur.hxj, dHy_k = cur.hy - hym, dHx_k = cur.hx - hxm;
+        const T cExy = ldg(&s.cExy[k]), cEyx = ldg(&s.cEyx[k]);
+        T ex = cur.ex, ey = cur.ey, ez = cur.ez;
+        const int id = cur.id;
+        if (id == CPS_ID_PEC) {
+            ex = T(0); ey = T(0); ez = T(0);
+        } else if (id != CPS_ID_DISPERSIVE) {
+            const T aE = ldg(&f.aE[id]), bE = ldg(&f.bE[id]);
+            ex = aE * ex + bE * dHz_j * cExz - bE * dHy_k * cExy;
+            ey = aE * ey + bE * dHx_k * cEyx - bE * dHz_i * cEyz;
+            ez = aE * ez + bE * dHy_i * cEzy - bE * dHx_j * cEzx;
         }
         if (DL) {
             const unsigned m = __ballot_sync(0xffffffffu, act && id == CPS_ID_DISPERSIVE);
@@ -155,8 +224,8 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
                 if (act && id == CPS_ID_DISPERSIVE) {
                     const int64_t c = base + __popc(m & lanemask_lt()), sc = D.ncell;
                     const T C3 = D.c.C3;
-                    const T cxx = C3 * dHz_j * cExz - C3 * dHy_k * s.cExy[k];
-                    const T cyy = C3 * dHx_k * s.cEyx[k] - C3 * dHz_i * cEyz;
+                    const T cxx = C3 * dHz_j * cExz - C3 * dHy_k * cExy;
+                    const T cyy = C3 * dHx_k * cEyx - C3 * dHz_i * cEyz;
                     const T czz = C3 * dHy_i * cEzy - C3 * dHx_j * cEzx;
                     T *st = D.state + c;
                     ex = dl_component(D.c, ex, cxx, st, sc);
@@ -171,20 +240,20 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
             if (m) {
                 const int64_t base = G.seg[((int64_t)k * (d.ny + 1) + j) * nseg + blockIdx.x];
                 if (mine) {
-                    using L = GainSite32;
                     const int64_t c = base + __popc(m & lanemask_lt()), sc = G.ncell;
                     T *st = G.state + c;
                     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
                     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
                     double N[4];
                     if (sizeof(T) == 8) {
-                        using L64 = GainSite64;
+                        using L = GainSite64;
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
-                            Pa[q] = st[(L64::PA + q) * sc]; Pa1[q] = st[(L64::PA1 + q) * sc];
-                            Pb[q] = st[(L64::PB + q) * sc]; Pb1[q] = st[(L64::PB1 + q) * sc];
+                            Pa[q] = st[(L::PA + q) * sc]; Pa1[q] = st[(L::PA1 + q) * sc];
+                            Pb[q] = st[(L::PB + q) * sc]; Pb1[q] = st[(L::PB1 + q) * sc];
                         }
                     } else {
+                        using L = GainSite32;
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
                             Pa[q] = st[(L::PA + q) * sc]; Pa1[q] = st[(L::PA1 + q) * sc];
@@ -197,14 +266,15 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
                     for (int q = 0; q < 3; ++q) E[q] = gain_e_corr<T>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
                     gain_n_update<T>(G.c, N, E, E1, Pa, Pa1, Pa2, Pb, Pb2);
                     if (sizeof(T) == 8) {
-                        using L64 = GainSite64;
+                        using L = GainSite64;
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
-                            st[(L64::PA + q) * sc] = Pa[q]; st[(L64::PA1 + q) * sc] = Pa1[q]; st[(L64::PA2 + q) * sc] = Pa2[q];
-                            st[(L64::PB + q) * sc] = Pb[q]; st[(L64::PB1 + q) * sc] = Pb1[q]; st[(L64::PB2 + q) * sc] = Pb2[q];
-                            st[(L64::E1 + q) * sc] = E1[q];
+                            st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q]; st[(L::PA2 + q) * sc] = Pa2[q];
+                            st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q]; st[(L::PB2 + q) * sc] = Pb2[q];
+                            st[(L::E1 + q) * sc] = E1[q];
                         }
                     } else {
+                        using L = GainSite32;
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
                             st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q];
@@ -221,7 +291,7 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
                 const T ce = p.cpmlE;
                 if (fx >= 0) {
                     const int np = p.np[fx];
-                    const int64_t q = ((int64_t)k * (d.ny + 1) + j) * (np + 1) + sxl;
+                    const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + sxl;
                     T *q0 = p.qe[fx][0], *q1 = p.qe[fx][1];
                     const T a0 = bx * q0[q] + cx * dHz_i, a1 = bx * q1[q] + cx * dHy_i;
                     q0[q] = a0; q1[q] = a1;
@@ -252,7 +322,8 @@ __global__ void __launch_bounds__(32 * BY) k_e_fused(FieldView<T> f, PmlView<T> 
             }
             f.Ex[g] = ex; f.Ey[g] = ey; f.Ez[g] = ez;
         }
-        hxm = hx; hym = hy;
+        hxm = cur.hx; hym = cur.hy;
+        cur = nxt;
     }
 }
 
@@ -292,7 +363,6 @@ template <typename T>
 void launch_h_fused(const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, cudaStream_t s)
 {
     switch (sh.by) {
-    case 2: h_fused_by<T, 2>(f, p, sh.kc, s); break;
     case 4: h_fused_by<T, 4>(f, p, sh.kc, s); break;
     case 16: h_fused_by<T, 16>(f, p, sh.kc, s); break;
     default: h_fused_by<T, 8>(f, p, sh.kc, s); break;
@@ -304,7 +374,6 @@ void launch_e_fused(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> 
                     FusedShape sh, cudaStream_t s)
 {
     switch (sh.by) {
-    case 2: e_fused_by<T, 2>(f, p, d, g, sh.kc, s); break;
     case 4: e_fused_by<T, 4>(f, p, d, g, sh.kc, s); break;
     case 16: e_fused_by<T, 16>(f, p, d, g, sh.kc, s); break;
     default: e_fused_by<T, 8>(f, p, d, g, sh.kc, s); break;

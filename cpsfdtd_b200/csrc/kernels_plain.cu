@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(32 * kBY) k_e_bulk(FieldView<T> f)
 // psi index of slab-local s at (i,j,k) for axis a (x: [k][j][s], y: [k][s][i], z: [s][j][i])
 __device__ __forceinline__ int64_t psi_index(const Dims &d, int axis, int np, int s, int i, int j, int k)
 {
-    if (axis == 0) return ((int64_t)k * (d.ny + 1) + j) * (np + 1) + s;
+    if (axis == 0) return ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + s;
     if (axis == 1) return ((int64_t)k * (np + 1) + s) * d.px + i;
     return ((int64_t)s * (d.ny + 1) + j) * d.px + i;
 }

@@ -14,12 +14,16 @@ namespace cps {
 
 namespace {
 
+// all ports of a grid in one launch: blockIdx.y selects the port
 template <typename T>
-__global__ void k_gather(FieldView<T> f, const int64_t *idx, int npts, T *slot)
+__global__ void k_gather(FieldView<T> f, GatherBatch b)
 {
+    const GatherDesc &q = b.p[blockIdx.y];
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int npts = q.npts;
     if (p >= npts) return;
-    const int64_t g = idx[p];
+    T *slot = (T *)q.slot;
+    const int64_t g = q.idx[p];
     slot[p] = f.Ex[g];
     slot[npts + p] = f.Ey[g];
     slot[2 * (int64_t)npts + p] = f.Ez[g];
@@ -28,62 +32,92 @@ __global__ void k_gather(FieldView<T> f, const int64_t *idx, int npts, T *slot)
     slot[5 * (int64_t)npts + p] = f.Hz[g];
 }
 
-// phasor table [t][f] = (cos, sin)(w_f * n_t * dt), FP64
-__global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_first, double dt, double *tab)
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
+// phasor table [t][f] = (cos, sin)(w_f * n_t * dt), phases in FP64, stored in
+// the contraction precision R
+template <typename R>
+__global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_first, double dt,
+                          typename Vec2<R>::type *tab)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nslots * nfreq) return;
     const int t = q / nfreq, fi = q - t * nfreq;
     double s, c;
     sincos(omega[fi] * ((double)(n_first + t) * dt), &s, &c);
-    tab[2 * q] = c;
-    tab[2 * q + 1] = s;
+    tab[q].x = (R)c;
+    tab[q].y = (R)s;
 }
 
-constexpr int kFch = 16;  // frequencies per thread
+// Register-tiled contraction: a block covers 64 points x 64 frequencies of
+// one component; each thread accumulates 4 points x 8 frequencies.  The
+// block's samples [slots][64] and phasors [slots][64] are staged in shared
+// memory.  Products and the sum over the (at most 64) slots of one flush run
+// in the sample precision T; the block sums are then added to the FP64
+// accumulators, H components rotated by exp(+i w dt/2) (they sit half a step
+// earlier).
+constexpr int kPT = 64, kFT = 64, kMaxSlots = 64;
 
-// one thread = one (point, component, 16-frequency chunk); blockIdx.y = component
 template <typename T>
-__global__ void __launch_bounds__(128) k_dft(const T *ring, int npts, int nslots, const double *tab,
-                                             const double *omega, int nfreq, double dt,
-                                             const int32_t *comps, double *acc)
+__global__ void __launch_bounds__(128) k_dft(const T *ring, int npts, int nslots,
+                                             const typename Vec2<T>::type *tab, const double *omega,
+                                             int nfreq, double dt, const int32_t *comps, double *acc)
 {
-    extern __shared__ double sh[];  // [nslots][kFch][2]
-    const int ci = blockIdx.y, f0 = blockIdx.z * kFch;
-    const int nf = min(kFch, nfreq - f0);
-    for (int q = threadIdx.x; q < nslots * kFch; q += blockDim.x) {
-        const int t = q / kFch, fi = q - t * kFch;
-        const bool ok = fi < nf;
-        sh[2 * q] = ok ? tab[2 * (t * nfreq + f0 + fi)] : 0.0;
-        sh[2 * q + 1] = ok ? tab[2 * (t * nfreq + f0 + fi) + 1] : 0.0;
+    using V = typename Vec2<T>::type;
+    extern __shared__ __align__(16) unsigned char sh_raw[];
+    T *ss = reinterpret_cast<T *>(sh_raw);                              // [nslots][kPT]
+    V *sp = reinterpret_cast<V *>(sh_raw + sizeof(T) * kMaxSlots * kPT);  // [nslots][kFT]
+    const int ci = blockIdx.y, p0 = blockIdx.x * kPT, f0 = blockIdx.z * kFT;
+    const int comp = comps[ci];
+    const int tid = threadIdx.x, tp = tid & 15, tf = tid >> 4;
+    for (int q = tid; q < nslots * kPT; q += blockDim.x) {
+        const int t = q / kPT, pl = q - t * kPT, p = p0 + pl;
+        ss[q] = p < npts ? ring[((int64_t)t * 6 + comp) * npts + p] : T(0);
+    }
+    for (int q = tid; q < nslots * kFT; q += blockDim.x) {
+        const int t = q / kFT, fl = q - t * kFT, f = f0 + fl;
+        V z;
+        z.x = T(0); z.y = T(0);
+        sp[q] = f < nfreq ? tab[(int64_t)t * nfreq + f] : z;
     }
     __syncthreads();
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= npts) return;
-    const int comp = comps[ci];
-    double re[kFch], im[kFch];
+    T re[4][8], im[4][8];
 #pragma unroll
-    for (int fi = 0; fi < kFch; ++fi) { re[fi] = 0.0; im[fi] = 0.0; }
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) { re[a][b] = T(0); im[a][b] = T(0); }
     for (int t = 0; t < nslots; ++t) {
-        const double v = (double)ring[((int64_t)t * 6 + comp) * npts + p];
-        const double *ph = sh + 2 * t * kFch;
+        T s[4];
 #pragma unroll
-        for (int fi = 0; fi < kFch; ++fi) {
-            re[fi] = fma(v, ph[2 * fi], re[fi]);
-            im[fi] = fma(-v, ph[2 * fi + 1], im[fi]);
+        for (int a = 0; a < 4; ++a) s[a] = ss[t * kPT + tp * 4 + a];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const V w = sp[t * kFT + tf * 8 + b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                re[a][b] = fma(s[a], w.x, re[a][b]);
+                im[a][b] = fma(-s[a], w.y, im[a][b]);
+            }
         }
     }
-    for (int fi = 0; fi < nf; ++fi) {
-        double r = re[fi], m = im[fi];
-        if (comp >= 3) {  // H sits half a step earlier: multiply by exp(+i w dt/2)
-            double sn, cs;
-            sincos(omega[f0 + fi] * (0.5 * dt), &sn, &cs);
-            const double r2 = r * cs - m * sn, m2 = r * sn + m * cs;
-            r = r2; m = m2;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const int f = f0 + tf * 8 + b;
+        if (f >= nfreq) continue;
+        double cs = 1.0, sn = 0.0;
+        if (comp >= 3) sincos(omega[f] * (0.5 * dt), &sn, &cs);
+        double *ar = acc + ((int64_t)(ci * nfreq + f) * 2) * npts;
+        double *ai = ar + npts;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int p = p0 + tp * 4 + a;
+            if (p >= npts) continue;
+            const double r = (double)re[a][b], m = (double)im[a][b];
+            ar[p] += r * cs - m * sn;
+            ai[p] += r * sn + m * cs;
         }
-        double *a = acc + ((int64_t)(ci * nfreq + f0 + fi) * 2) * npts + p;
-        a[0] += r;
-        a[npts] += m;
     }
 }
 
@@ -150,10 +184,10 @@ inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b);
 }  // namespace
 
 template <typename T>
-void launch_port_gather(const FieldView<T> &f, const int64_t *idx, int npts, T *slot, cudaStream_t s)
+void launch_port_gather(const FieldView<T> &f, const GatherBatch &b, cudaStream_t s)
 {
-    if (npts <= 0) return;
-    k_gather<T><<<cdiv(npts, 256), 256, 0, s>>>(f, idx, npts, slot);
+    if (b.n <= 0 || b.max_npts <= 0) return;
+    k_gather<T><<<dim3(cdiv(b.max_npts, 256), b.n), 256, 0, s>>>(f, b);
 }
 
 template <typename T>
@@ -162,10 +196,17 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
                      cudaStream_t s)
 {
     if (npts <= 0 || nslots <= 0 || nfreq <= 0 || ncomp <= 0) return;
-    k_phasors<<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, scratch_phasor);
-    dim3 grid(cdiv(npts, 128), ncomp, cdiv(nfreq, kFch));
-    const size_t smem = sizeof(double) * 2 * kFch * nslots;
-    k_dft<T><<<grid, 128, smem, s>>>(ring, npts, nslots, scratch_phasor, omega, nfreq, dt, comps, acc);
+    using V = typename Vec2<T>::type;
+    V *tab = reinterpret_cast<V *>(scratch_phasor);
+    k_phasors<T><<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, tab);
+    dim3 grid(cdiv(npts, kPT), ncomp, cdiv(nfreq, kFT));
+    const size_t smem = (sizeof(T) * kPT + sizeof(V) * kFT) * kMaxSlots;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_dft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_dft<T><<<grid, 128, smem, s>>>(ring, npts, nslots, tab, omega, nfreq, dt, comps, acc);
 }
 
 void launch_port_flux(const double *acc, int npts, int nfreq, int ncomp, const int32_t *sel, double dA,
@@ -197,7 +238,7 @@ void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s
 }
 
 #define CPS_INST(T)                                                                                        \
-    template void launch_port_gather<T>(const FieldView<T> &, const int64_t *, int, T *, cudaStream_t);    \
+    template void launch_port_gather<T>(const FieldView<T> &, const GatherBatch &, cudaStream_t);          \
     template void launch_port_dft<T>(const T *, int, int, int64_t, double, const double *, int,            \
                                      const int32_t *, int, double *, double *, cudaStream_t);              \
     template void launch_count_nonfinite<T>(const FieldView<T> &, unsigned long long *, cudaStream_t);     \

@@ -261,6 +261,14 @@ CPS_API cps_status cps_ports_flush(cps_grid *g);
  * samples); cps_grid_timing synchronises and returns their mean durations in
  * milliseconds.  stride 0 turns it off and clears the samples. */
 CPS_API cps_status cps_grid_set_timing(cps_grid *g, int32_t stride);
+/* tile of the fused sweeps: rows (4, 8 or 16) of 32 columns per block and
+ * planes marched per block (>= 1); the default is 4 rows x 8 planes */
+CPS_API cps_status cps_grid_set_tile(cps_grid *g, int32_t rows, int32_t planes);
+CPS_API cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *planes);
+/* fused sweep kind: 0 (default) stages x-y tiles of several planes in shared
+ * memory with TMA bulk-tensor loads (tiles of 4 or 8 rows); 1 loads through
+ * registers.  Both give the same results. */
+CPS_API cps_status cps_grid_set_sweep(cps_grid *g, int32_t mode);
 CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sweep_ms, int64_t *samples);
 
 #ifdef __cplusplus

@@ -98,3 +98,24 @@ def test_gain_populations_match_oracle(oracle_mod, oracle_runs):
         assert got.shape == want.shape
         assert np.abs(got - want).max() <= tol
         assert np.abs(got.sum(axis=1) - 2.0).max() < 1e-12  # conservation, FourLevelLaser.cpp:324
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32"])
+def test_tma_and_register_sweeps_agree(prec):
+    """The TMA-fed sweeps (default) and the register sweeps compute the same
+    update; on a grid wide enough for the TMA boxes they agree to rounding."""
+    import cpsfdtd_b200 as cps
+    dk = decks.config2(n=72, steps=80, nfreq=4)
+    ids = cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    out = []
+    for mode, rows in ((0, 8), (0, 4), (1, 8)):
+        g = cps.Grid.from_deck(dk, prec, ids=ids)
+        g.set_sweep(mode)
+        g.set_tile(rows, 16)
+        g.step(dk.nsteps, cps.FUSED)
+        g.sync()
+        out.append([g.field(c) for c in range(6)] + [g.port_dft(0)])
+    tol = 1e-12 if prec == 0 else 1e-5
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert rel_l2(a, b) < tol
