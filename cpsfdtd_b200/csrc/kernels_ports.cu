@@ -51,23 +51,25 @@ __global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_
     tab[q].y = (R)s;
 }
 
-// Register-tiled contraction: a block covers 64 points x 64 frequencies of
-// one component; each thread accumulates 4 points x 8 frequencies.  The
-// block's samples [slots][64] and phasors [slots][64] are staged in shared
-// memory.  Products and the sum over the (at most 64) slots of one flush run
-// in the sample precision T; the block sums are then added to the FP64
-// accumulators, H components rotated by exp(+i w dt/2) (they sit half a step
-// earlier).
+// Register-tiled contraction: a block of 256 threads covers 64 points x 64
+// frequencies of one component; thread (tp, tf) accumulates points
+// p0 + 16a + tp (a = 0..3) at frequencies f0 + 4tf + b (b = 0..3), so
+// neighbouring lanes touch neighbouring points in shared memory and in the
+// FP64 accumulators.  The block's samples [slots][64] and phasors
+// [slots][64] are staged in shared memory.  Products and the sum over the
+// (at most 64) slots of one flush run in the sample precision T; the block
+// sums are then added to the FP64 accumulators, H components rotated by
+// exp(+i w dt/2) (they sit half a step earlier).
 constexpr int kPT = 64, kFT = 64, kMaxSlots = 64;
 
 template <typename T>
-__global__ void __launch_bounds__(128) k_dft(const T *ring, int npts, int nslots,
+__global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots,
                                              const typename Vec2<T>::type *tab, const double *omega,
                                              int nfreq, double dt, const int32_t *comps, double *acc)
 {
     using V = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char sh_raw[];
-    T *ss = reinterpret_cast<T *>(sh_raw);                              // [nslots][kPT]
+    T *ss = reinterpret_cast<T *>(sh_raw);                                // [nslots][kPT]
     V *sp = reinterpret_cast<V *>(sh_raw + sizeof(T) * kMaxSlots * kPT);  // [nslots][kFT]
     const int ci = blockIdx.y, p0 = blockIdx.x * kPT, f0 = blockIdx.z * kFT;
     const int comp = comps[ci];
@@ -83,28 +85,28 @@ __global__ void __launch_bounds__(128) k_dft(const T *ring, int npts, int nslots
         sp[q] = f < nfreq ? tab[(int64_t)t * nfreq + f] : z;
     }
     __syncthreads();
-    T re[4][8], im[4][8];
+    T re[4][4], im[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 8; ++b) { re[a][b] = T(0); im[a][b] = T(0); }
+        for (int b = 0; b < 4; ++b) { re[a][b] = T(0); im[a][b] = T(0); }
     for (int t = 0; t < nslots; ++t) {
-        T s[4];
+        T sv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) s[a] = ss[t * kPT + tp * 4 + a];
+        for (int a = 0; a < 4; ++a) sv[a] = ss[t * kPT + a * 16 + tp];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const V w = sp[t * kFT + tf * 8 + b];
+        for (int b = 0; b < 4; ++b) {
+            const V w = sp[t * kFT + tf * 4 + b];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                re[a][b] = fma(s[a], w.x, re[a][b]);
-                im[a][b] = fma(-s[a], w.y, im[a][b]);
+                re[a][b] = fma(sv[a], w.x, re[a][b]);
+                im[a][b] = fma(-sv[a], w.y, im[a][b]);
             }
         }
     }
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const int f = f0 + tf * 8 + b;
+    for (int b = 0; b < 4; ++b) {
+        const int f = f0 + tf * 4 + b;
         if (f >= nfreq) continue;
         double cs = 1.0, sn = 0.0;
         if (comp >= 3) sincos(omega[f] * (0.5 * dt), &sn, &cs);
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(128) k_dft(const T *ring, int npts, int nslots
         double *ai = ar + npts;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const int p = p0 + tp * 4 + a;
+            const int p = p0 + a * 16 + tp;
             if (p >= npts) continue;
             const double r = (double)re[a][b], m = (double)im[a][b];
             ar[p] += r * cs - m * sn;
@@ -206,7 +208,7 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
         cudaFuncSetAttribute(k_dft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_dft<T><<<grid, 128, smem, s>>>(ring, npts, nslots, tab, omega, nfreq, dt, comps, acc);
+    k_dft<T><<<grid, 256, smem, s>>>(ring, npts, nslots, tab, omega, nfreq, dt, comps, acc);
 }
 
 void launch_port_flux(const double *acc, int npts, int nfreq, int ncomp, const int32_t *sel, double dA,

@@ -49,14 +49,11 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bar, uint32_t phase)
 }
 
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
-__global__ void __launch_bounds__(32 * BY) k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
-                                                    DlView<T> D, GainView<T> G, int kc, int *err)
+__device__ __forceinline__ void e_tma_body(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p,
+                                           const DlView<T> &D, const GainView<T> &G, int kc, int *err,
+                                           unsigned char *sm, uint64_t *full)
 {
     using L = StageLayout<T, BY>;
-    extern __shared__ __align__(128) unsigned char sm_raw[];
-    __shared__ __align__(8) uint64_t full[kStages];
-    // TMA destinations 128-byte aligned in the shared window (SMEM holds 128 spare bytes)
-    unsigned char *sm = sm_raw + (((smem_u32(sm_raw) + 127u) & ~127u) - smem_u32(sm_raw));
     const Dims d = f.d;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * BY;
@@ -143,14 +140,10 @@ __global__ void __launch_bounds__(32 * BY) k_e_tma(const __grid_constant__ TmaMa
 }
 
 template <typename T, int BY, bool PML>
-__global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
-                                                    int kc, int *err)
+__device__ __forceinline__ void h_tma_body(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc,
+                                           int *err, unsigned char *sm, uint64_t *full)
 {
     using L = StageLayout<T, BY>;
-    extern __shared__ __align__(128) unsigned char sm_raw[];
-    __shared__ __align__(8) uint64_t full[kStages];
-    // TMA destinations 128-byte aligned in the shared window (SMEM holds 128 spare bytes)
-    unsigned char *sm = sm_raw + (((smem_u32(sm_raw) + 127u) & ~127u) - smem_u32(sm_raw));
     const Dims d = f.d;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * BY;
@@ -228,6 +221,49 @@ __global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMa
         __syncthreads();
         if (tid == 0 && k + kStages <= k1) issue(s, k + kStages);
     }
+}
+
+
+// Does a block's tile (32 columns from x0, BY rows from y0, planes [k0, k1))
+// meet a CPML slab?  E side: slabs [1, np] and [n-np, n-1]; H side: [0, np-1]
+// and [n-np, n-1] on each axis.  Blocks that do not run the CPML-free body.
+__device__ __forceinline__ bool tile_in_pml(const int np[6], const Dims &d, int x0, int y0, int by, int k0, int k1,
+                                            bool eside)
+{
+    const int lo = eside ? 0 : 1;  // first-end slab reaches index np (E) or np-1 (H)
+    const bool x = x0 <= np[kFX1] - lo || x0 + 31 >= d.nx - np[kFX2];
+    const bool y = y0 <= np[kFY1] - lo || y0 + by - 1 >= d.ny - np[kFY2];
+    const bool z = k0 <= np[kFZ1] - lo || k1 - 1 >= d.nz - np[kFZ2];
+    return x || y || z;
+}
+
+template <typename T, int BY, bool PML, bool DL, bool GAIN>
+__global__ void __launch_bounds__(32 * BY) k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
+                                                    DlView<T> D, GainView<T> G, int kc, int *err)
+{
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ __align__(8) uint64_t full[kStages];
+    // TMA destinations 128-byte aligned in the shared window (SMEM holds 128 spare bytes)
+    unsigned char *sm = sm_raw + (((smem_u32(sm_raw) + 127u) & ~127u) - smem_u32(sm_raw));
+    const int k0 = max(1, (int)blockIdx.z * kc), k1 = min((int)blockIdx.z * kc + kc, f.d.nz);
+    if (PML && tile_in_pml(p.np, f.d, blockIdx.x * 32, blockIdx.y * BY, BY, k0, k1, true))
+        e_tma_body<T, BY, true, DL, GAIN>(M, f, p, D, G, kc, err, sm, full);
+    else
+        e_tma_body<T, BY, false, DL, GAIN>(M, f, p, D, G, kc, err, sm, full);
+}
+
+template <typename T, int BY, bool PML>
+__global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
+                                                    int kc, int *err)
+{
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ __align__(8) uint64_t full[kStages];
+    unsigned char *sm = sm_raw + (((smem_u32(sm_raw) + 127u) & ~127u) - smem_u32(sm_raw));
+    const int k0 = (int)blockIdx.z * kc, k1 = min(k0 + kc, f.d.nz);
+    if (PML && tile_in_pml(p.np, f.d, blockIdx.x * 32, blockIdx.y * BY, BY, k0, k1, false))
+        h_tma_body<T, BY, true>(M, f, p, kc, err, sm, full);
+    else
+        h_tma_body<T, BY, false>(M, f, p, kc, err, sm, full);
 }
 
 // The ID-2 cells the TMA E sweep leaves alone: Drude-Lorentz ADE update
