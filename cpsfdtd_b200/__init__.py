@@ -18,7 +18,7 @@ from typing import Optional
 
 import numpy as np
 
-__all__ = ["Grid", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
+__all__ = ["Grid", "Batch", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcpsfdtd.so")
@@ -124,6 +124,15 @@ def lib():
             "cps_grid_set_tile": ([P, I32, I32], I32), "cps_grid_get_tile": ([P, ip, ip], I32),
             "cps_grid_set_sweep": ([P, I32], I32),
             "cps_grid_timing": ([P, C.POINTER(D), C.POINTER(D), C.POINTER(I64)], I32),
+            "cps_batch_create": ([I32, C.POINTER(P)], I32), "cps_batch_destroy": ([P], I32),
+            "cps_batch_add": ([P, P], I32), "cps_batch_remove": ([P, P], I32),
+            "cps_batch_info": ([P, ip, C.POINTER(I64)], I32), "cps_batch_step": ([P, I32], I32),
+            "cps_batch_synchronize": ([P], I32), "cps_batch_set_tile": ([P, I32, I32, I32], I32),
+            "cps_batch_get_tile": ([P, ip, ip, ip], I32), "cps_batch_set_graph": ([P, I32], I32),
+            "cps_batch_get_stream": ([P, C.POINTER(P)], I32),
+            "cps_batch_launch_count": ([P, C.POINTER(I64)], I32),
+            "cps_batch_tune_key": ([P, C.c_char_p, I32], I32),
+            "cps_batch_autotune": ([P, C.c_char_p, I32, ip], I32),
         }
         for name, (args, res) in sigs.items():
             fn = getattr(L, name)
@@ -389,3 +398,79 @@ class Grid:
         p = C.c_void_p()
         _check(self.L.cps_grid_get_stream(self.h, C.byref(p)))
         return p.value
+
+
+class Batch:
+    """Many grids of one precision advanced together by the batched engine
+    (``cps_batch_*``): one launch per sweep class over all members' tiles,
+    step chunks replayed as CUDA graphs.  Members stay ordinary
+    :class:`Grid` objects for set-up and read-out."""
+
+    def __init__(self, precision=FP32):
+        self.L = lib()
+        self.h = C.c_void_p()
+        _check(self.L.cps_batch_create(precision, C.byref(self.h)))
+        self.members = []
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.cps_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, g: Grid):
+        _check(self.L.cps_batch_add(self.h, g.h))
+        self.members.append(g)
+
+    def remove(self, g: Grid):
+        _check(self.L.cps_batch_remove(self.h, g.h))
+        self.members.remove(g)
+
+    def info(self):
+        n, c = C.c_int32(), C.c_int64()
+        _check(self.L.cps_batch_info(self.h, C.byref(n), C.byref(c)))
+        return n.value, c.value
+
+    def step(self, n=1):
+        _check(self.L.cps_batch_step(self.h, n))
+
+    def sync(self):
+        _check(self.L.cps_batch_synchronize(self.h))
+
+    def set_tile(self, rows, planes, persistent=0):
+        _check(self.L.cps_batch_set_tile(self.h, rows, planes, persistent))
+
+    def get_tile(self):
+        r, p, q = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(self.L.cps_batch_get_tile(self.h, C.byref(r), C.byref(p), C.byref(q)))
+        return r.value, p.value, q.value
+
+    def set_graph(self, on):
+        _check(self.L.cps_batch_set_graph(self.h, 1 if on else 0))
+
+    def stream(self):
+        s = C.c_void_p()
+        _check(self.L.cps_batch_get_stream(self.h, C.byref(s)))
+        return s.value
+
+    def launches(self):
+        n = C.c_int64()
+        _check(self.L.cps_batch_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    def tune_key(self):
+        buf = C.create_string_buffer(256)
+        _check(self.L.cps_batch_tune_key(self.h, buf, 256))
+        return buf.value.decode()
+
+    def autotune(self, cache_path="", trial_steps=4):
+        """Pick the tiling (cached per key in ``cache_path``); returns the
+        number of steps every member advanced while trying candidates."""
+        ran = C.c_int32()
+        _check(self.L.cps_batch_autotune(self.h, cache_path.encode(), trial_steps, C.byref(ran)))
+        return ran.value

@@ -32,6 +32,8 @@ SOURCES = {
     "kernels_fused.cu": [],
     "kernels_tma.cu": [],
     "kernels_ports.cu": [],
+    "kernels_batch.cu": [],
+    "batch.cpp": ["-x", "cu"],
 }
 
 

@@ -14,7 +14,7 @@
 #include <string>
 #include <vector>
 
-#include "cps_internal.h"
+#include "grid.h"
 
 namespace cps {
 
@@ -28,127 +28,8 @@ using namespace cps;
 extern "C" const char *cps_last_error(void) { return g_last_error.c_str(); }
 extern "C" const char *cps_version(void) { return "cpsfdtd-b200 0.1 (sm_100a)"; }
 
-#define CK(call)                                                                                   \
-    do {                                                                                           \
-        cudaError_t e_ = (call);                                                                   \
-        if (e_ != cudaSuccess) {                                                                   \
-            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                         \
-            return e_ == cudaErrorMemoryAllocation ? CPS_E_NOMEM : CPS_E_CUDA;                     \
-        }                                                                                          \
-    } while (0)
 
-#define REQUIRE(cond, code, msg)                                                                   \
-    do {                                                                                           \
-        if (!(cond)) {                                                                             \
-            set_error(msg);                                                                        \
-            return code;                                                                           \
-        }                                                                                          \
-    } while (0)
-
-namespace {
-
-struct PortState {
-    int npts = 0;
-    std::vector<int32_t> ijk;
-    int64_t *d_idx = nullptr;
-    void *d_ring = nullptr;  // [slots][6][npts] of T
-    int slots = 1;
-    int fill = 0;            // samples in the ring not yet folded into the DFT
-    int64_t ring_n0 = 0;     // step of ring slot 0
-    int last_slot = -1;
-    int nfreq = 0;
-    uint32_t mask = 0;
-    int ncomp = 0;
-    int comps[6] = {0, 0, 0, 0, 0, 0};
-    int32_t *d_comps = nullptr;
-    double *d_omega = nullptr;
-    double *d_acc = nullptr;  // [ncomp][nfreq][2][npts]
-};
-
-struct Src {
-    int comp;
-    int64_t idx;
-    std::vector<double> wave;
-};
-
-}  // namespace
-
-struct cps_grid {
-    cps_grid_desc desc{};
-    bool fp32 = false;
-    size_t esz = 8;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    Dims d{};
-    int64_t elems = 0;  // device elements per field array
-    void *F[6] = {};
-    uint8_t *d_id = nullptr;
-    std::vector<uint8_t> ids_dev;  // host copy in device order
-    bool ids_set = false;
-    int nmedia = 0;
-    double aE[256] = {}, bE[256] = {}, aH[256] = {}, bH[256] = {};
-    void *d_media = nullptr;  // aE bE aH bH, 256 each, of T
-    std::vector<double> st[12];
-    void *d_st = nullptr;
-    // CPML
-    bool pml_on = false;
-    cps_pml_params pml{};
-    std::vector<double> pbE[6], pcE[6], pbH[6], pcH[6];
-    void *d_pcoef = nullptr;
-    void *d_q[6][4] = {};
-    double cpmlE = 0, cpmlH = 0;
-    // Drude-Lorentz
-    bool dl_on = false;
-    DlCoef<double> dlc{};
-    int64_t dl_n = 0;
-    int64_t *d_dl_cell = nullptr;
-    int32_t *d_dl_seg = nullptr;
-    void *d_dl_state = nullptr;
-    // gain
-    bool gain_on = false;
-    GainCoef gc{};
-    int gain_id = 5;
-    int64_t g_n = 0;
-    int64_t *d_g_cell = nullptr;
-    int32_t *d_g_seg = nullptr;
-    void *d_g_state = nullptr;
-    // TF/SF
-    bool tfsf_on = false;
-    cps_tfsf_params tp{};
-    std::vector<double> einc, hinc;
-    void *d_einc = nullptr, *d_hinc = nullptr;
-    InjTarget *d_tg[2] = {nullptr, nullptr};   // 0: E targets, 1: H targets
-    InjContrib *d_ct[2] = {nullptr, nullptr};
-    int ntg[2] = {0, 0};
-    // sources
-    std::vector<Src> src;
-    int64_t *d_src_idx = nullptr;
-    int32_t *d_src_comp = nullptr, *d_src_off = nullptr, *d_src_len = nullptr;
-    double *d_src_wave = nullptr;
-    bool src_dirty = false;
-    // ports
-    std::vector<PortState> ports;
-    double *d_phasor = nullptr;
-    size_t phasor_cap = 0;
-    // misc
-    int64_t step = 1;
-    int64_t launches = 0;
-    FusedShape shape{4, 8};
-    double *d_conv = nullptr;
-    unsigned long long *d_counter = nullptr;
-    // TMA tensor maps of the fused sweeps (built for tile rows tma_by)
-    TmaMaps tma{};
-    int tma_by = 0;
-    int sweep_mode = 0;  // 0: TMA-fed sweeps, 1: register sweeps
-    int *d_err = nullptr;  // set by a device wait that gave up
-    // sweep timing samples: events (start, after H sweep, after E sweep)
-    int timing_stride = 0;
-    std::vector<cudaEvent_t> ev;
-    int ev_used = 0;
-    std::vector<std::pair<void *, size_t>> owned;  // every device allocation and its size
-};
-
-namespace {
+namespace cps {
 
 cps_status dalloc(cps_grid *g, void **p, size_t bytes)
 {
@@ -196,13 +77,6 @@ cps_status upload_raw(cps_grid *g, void *dst, const void *src, size_t bytes)
     return CPS_OK;
 }
 
-const int kStretchLen(const cps_grid *g, int w)
-{
-    const int n[12] = {g->d.nz, g->d.nz, g->d.ny, g->d.ny, g->d.nx, g->d.nx,
-                       g->d.nz, g->d.nz, g->d.ny, g->d.ny, g->d.nx, g->d.nx};
-    return n[w];
-}
-
 // stretch arrays on the device: 12 arrays packed, each padded to 8 entries
 cps_status push_stretch(cps_grid *g)
 {
@@ -216,91 +90,6 @@ cps_status push_stretch(cps_grid *g)
         if (s) return s;
     }
     return upload_real(g, g->d_st, all.data(), all.size());
-}
-
-template <typename T>
-StretchView<T> stretch_view(const cps_grid *g)
-{
-    StretchView<T> v;
-    const T *base = (const T *)g->d_st;
-    const T *a[12];
-    size_t off = 0;
-    for (int w = 0; w < 12; ++w) {
-        a[w] = base + off;
-        off += (size_t)(kStretchLen(g, w) + 7) / 8 * 8;
-    }
-    v.cExy = a[0]; v.cEyx = a[1]; v.cEzx = a[2]; v.cExz = a[3]; v.cEzy = a[4]; v.cEyz = a[5];
-    v.cHxy = a[6]; v.cHyx = a[7]; v.cHzx = a[8]; v.cHxz = a[9]; v.cHzy = a[10]; v.cHyz = a[11];
-    return v;
-}
-
-template <typename T>
-FieldView<T> field_view(const cps_grid *g)
-{
-    FieldView<T> f;
-    f.d = g->d;
-    f.Ex = (T *)g->F[0]; f.Ey = (T *)g->F[1]; f.Ez = (T *)g->F[2];
-    f.Hx = (T *)g->F[3]; f.Hy = (T *)g->F[4]; f.Hz = (T *)g->F[5];
-    f.id = g->d_id;
-    const T *m = (const T *)g->d_media;
-    f.aE = m; f.bE = m + 256; f.aH = m + 512; f.bH = m + 768;
-    f.s = stretch_view<T>(g);
-    return f;
-}
-
-template <typename T>
-PmlView<T> pml_view(const cps_grid *g)
-{
-    PmlView<T> p;
-    memset(&p, 0, sizeof(p));
-    p.on = g->pml_on;
-    if (!g->pml_on) return p;
-    const T *c = (const T *)g->d_pcoef;
-    size_t off = 0;
-    for (int f = 0; f < 6; ++f) {
-        p.np[f] = g->pml.npml[f];
-        const size_t n = (size_t)p.np[f] + 1;
-        p.bE[f] = c + off; off += n;
-        p.cE[f] = c + off; off += n;
-        p.bH[f] = c + off; off += n;
-        p.cH[f] = c + off; off += n;
-        p.qe[f][0] = (T *)g->d_q[f][0]; p.qe[f][1] = (T *)g->d_q[f][1];
-        p.qh[f][0] = (T *)g->d_q[f][2]; p.qh[f][1] = (T *)g->d_q[f][3];
-    }
-    p.cpmlE = (T)g->cpmlE;
-    p.cpmlH = (T)g->cpmlH;
-    return p;
-}
-
-template <typename T>
-DlView<T> dl_view(const cps_grid *g)
-{
-    DlView<T> v;
-    memset(&v, 0, sizeof(v));
-    v.on = g->dl_on;
-    if (!g->dl_on) return v;
-    v.ncell = g->dl_n; v.cell = g->d_dl_cell; v.seg = g->d_dl_seg; v.state = (T *)g->d_dl_state;
-    const DlCoef<double> &c = g->dlc;
-    v.c.nD = c.nD; v.c.nL = c.nL; v.c.stride = c.stride;
-    v.c.C1 = (T)c.C1; v.c.C2 = (T)c.C2; v.c.C3 = (T)c.C3; v.c.dt = (T)c.dt; v.c.inv2dt = (T)c.inv2dt;
-    for (int p = 0; p < kMaxPoles; ++p) {
-        v.c.kappa[p] = (T)c.kappa[p]; v.c.beta[p] = (T)c.beta[p]; v.c.C4[p] = (T)c.C4[p];
-        v.c.alpha[p] = (T)c.alpha[p]; v.c.xi[p] = (T)c.xi[p]; v.c.gammaL[p] = (T)c.gammaL[p];
-        v.c.C5[p] = (T)c.C5[p]; v.c.C6[p] = (T)c.C6[p];
-    }
-    return v;
-}
-
-template <typename T>
-GainView<T> gain_view(const cps_grid *g)
-{
-    GainView<T> v;
-    memset(&v, 0, sizeof(v));
-    v.on = g->gain_on;
-    if (!g->gain_on) return v;
-    v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg;
-    v.state = (T *)g->d_g_state; v.c = g->gc;
-    return v;
 }
 
 // ------------------------------------------------------------ CPML coefs
@@ -485,7 +274,7 @@ template <typename T>
 cps_status flush_dft_T(cps_grid *g, PortState &P)
 {
     if (P.nfreq == 0 || P.fill == 0) return CPS_OK;
-    const size_t need = (size_t)P.slots * P.nfreq * 2 * sizeof(double);
+    const size_t need = (size_t)2 * P.slots * P.nfreq * 2 * sizeof(double);  // [2][slots][nfreq] of (cos, sin)
     if (g->phasor_cap < need) {
         dfree(g, g->d_phasor);
         cps_status s = dalloc(g, (void **)&g->d_phasor, need);
@@ -638,7 +427,7 @@ cps_status need_setup(const cps_grid *g)
     return CPS_OK;
 }
 
-}  // namespace
+}  // namespace cps
 
 // ================================================================ lifetime
 

@@ -1,0 +1,253 @@
+// kernels_batch.cu -- sweeps and Drude-Lorentz cells of many grids in one
+// launch (sm_100a).  A block takes tiles from a flat table, each naming its
+// grid, and runs the same per-tile bodies as the one-grid kernels
+// (tma_bodies.cuh), so a cell's arithmetic does not depend on which launch,
+// tile shape or co-resident grids processed it.  With fewer blocks than
+// tiles a block walks the table with a stride of the grid size (persistent
+// launch); its stage ring and mbarriers carry over from tile to tile.
+//
+// The tensor maps live in the descriptor table in device memory, written by
+// the host before the launch; the issuing thread orders its TMA reads after
+// those writes with fence.proxy.tensormap::generic.acquire whenever it moves
+// to another grid's maps.  No multicast is used.
+#include <cuda.h>
+
+#include "batch.h"
+#include "tma_bodies.cuh"
+
+namespace cps {
+
+namespace {
+
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.sys [%0], 128;" ::"l"(reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
+__device__ __forceinline__ void acquire_maps(const TmaMaps &M)
+{
+    for (int c = 0; c < 6; ++c) {
+        tensormap_acquire(&M.halo[c]);
+        tensormap_acquire(&M.own[c]);
+    }
+    tensormap_acquire(&M.id);
+}
+
+template <typename T, int BY, bool PML>
+__global__ void __launch_bounds__(32 * BY) k_h_batch(const BatchGrid<T> *__restrict__ grids,
+                                                      const int4 *__restrict__ tiles, int ntiles, int *err)
+{
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ __align__(8) uint64_t full[kStages];
+    unsigned char *sm = align_smem(sm_raw);
+    init_stages(full);
+    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+    uint32_t ctr = 0;
+    int last = -1;
+    for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
+        const int4 e = tiles[q];
+        const BatchGrid<T> &B = grids[e.x];
+        if (e.x != last) {
+            if (lead) acquire_maps(B.M);
+            last = e.x;
+        }
+        if (!h_tma_body<T, BY, PML>(B.M, B.f, B.p, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm, full)) return;
+    }
+}
+
+template <typename T, int BY, bool PML, bool GAIN>
+__global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restrict__ grids,
+                                                      const int4 *__restrict__ tiles, int ntiles, int *err)
+{
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ __align__(8) uint64_t full[kStages];
+    unsigned char *sm = align_smem(sm_raw);
+    init_stages(full);
+    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+    uint32_t ctr = 0;
+    int last = -1;
+    for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
+        const int4 e = tiles[q];
+        const BatchGrid<T> &B = grids[e.x];
+        if (e.x != last) {
+            if (lead) acquire_maps(B.M);
+            last = e.x;
+        }
+        const TileXYZ t{e.y, e.z, e.w};
+        bool ok;
+        if (B.D.on && B.D.ncell > 0)
+            ok = e_tma_body<T, BY, PML, true, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, t, ctr, err, sm, full);
+        else
+            ok = e_tma_body<T, BY, PML, false, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, t, ctr, err, sm, full);
+        if (!ok) return;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_dl_batch(const BatchGrid<T> *__restrict__ grids,
+                                                  const int4 *__restrict__ blocks)
+{
+    const int4 e = blocks[blockIdx.x];
+    const int64_t c = (int64_t)e.y + threadIdx.x;
+    if (c >= e.z) return;
+    const BatchGrid<T> &B = grids[e.x];
+    if (B.p.on) dl_cell<T, true>(B.f, B.p, B.D, c);
+    else dl_cell<T, false>(B.f, B.p, B.D, c);
+}
+
+template <typename T>
+__global__ void k_advance(BatchGrid<T> *grids, int ngrids, int nsteps)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < ngrids) grids[g].n0 += nsteps;
+}
+
+inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+template <auto K>
+void smem_attr(int bytes)
+{
+    static bool done = false;  // one flag per kernel
+    if (!done) {
+        cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        done = true;
+    }
+}
+
+template <typename T, int BY, bool PML>
+void h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
+{
+    using L = StageLayout<T, BY>;
+    smem_attr<k_h_batch<T, BY, PML>>(L::SMEM);
+    k_h_batch<T, BY, PML><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
+}
+
+template <typename T, int BY, bool PML, bool GAIN>
+void e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
+{
+    using L = StageLayout<T, BY>;
+    smem_attr<k_e_batch<T, BY, PML, GAIN>>(L::SMEM);
+    k_e_batch<T, BY, PML, GAIN><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
+}
+
+template <typename K>
+int occupancy(K kernel, int threads, int smem)
+{
+    int n = 0;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+}  // namespace
+
+template <typename T>
+void launch_h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, bool pml,
+                    int *err, cudaStream_t s)
+{
+    if (ntiles <= 0) return;
+    if (nblocks <= 0 || nblocks > ntiles) nblocks = ntiles;
+    if (by == 4) {
+        if (pml) h_batch<T, 4, true>(grids, tiles, ntiles, nblocks, err, s);
+        else h_batch<T, 4, false>(grids, tiles, ntiles, nblocks, err, s);
+    } else {
+        if (pml) h_batch<T, 8, true>(grids, tiles, ntiles, nblocks, err, s);
+        else h_batch<T, 8, false>(grids, tiles, ntiles, nblocks, err, s);
+    }
+}
+
+template <typename T>
+void launch_e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, bool pml,
+                    bool gain, int *err, cudaStream_t s)
+{
+    if (ntiles <= 0) return;
+    if (nblocks <= 0 || nblocks > ntiles) nblocks = ntiles;
+    if (by == 4) {
+        if (pml) {
+            if (gain) e_batch<T, 4, true, true>(grids, tiles, ntiles, nblocks, err, s);
+            else e_batch<T, 4, true, false>(grids, tiles, ntiles, nblocks, err, s);
+        } else {
+            if (gain) e_batch<T, 4, false, true>(grids, tiles, ntiles, nblocks, err, s);
+            else e_batch<T, 4, false, false>(grids, tiles, ntiles, nblocks, err, s);
+        }
+    } else {
+        if (pml) {
+            if (gain) e_batch<T, 8, true, true>(grids, tiles, ntiles, nblocks, err, s);
+            else e_batch<T, 8, true, false>(grids, tiles, ntiles, nblocks, err, s);
+        } else {
+            if (gain) e_batch<T, 8, false, true>(grids, tiles, ntiles, nblocks, err, s);
+            else e_batch<T, 8, false, false>(grids, tiles, ntiles, nblocks, err, s);
+        }
+    }
+}
+
+template <typename T>
+void launch_dl_batch(const BatchGrid<T> *grids, const int4 *blocks, int nblocks, cudaStream_t s)
+{
+    if (nblocks <= 0) return;
+    k_dl_batch<T><<<nblocks, 128, 0, s>>>(grids, blocks);
+}
+
+template <typename T>
+void launch_advance_batch(BatchGrid<T> *grids, int ngrids, int nsteps, cudaStream_t s)
+{
+    if (ngrids <= 0) return;
+    k_advance<T><<<cdiv(ngrids, 128), 128, 0, s>>>(grids, ngrids, nsteps);
+}
+
+template <typename T>
+int batch_blocks_per_sm(int by, bool eside, bool pml, bool gain)
+{
+    if (by == 4) {
+        using L = StageLayout<T, 4>;
+        if (!eside) return pml ? occupancy(k_h_batch<T, 4, true>, 128, L::SMEM)
+                               : occupancy(k_h_batch<T, 4, false>, 128, L::SMEM);
+        if (pml) return gain ? occupancy(k_e_batch<T, 4, true, true>, 128, L::SMEM)
+                             : occupancy(k_e_batch<T, 4, true, false>, 128, L::SMEM);
+        return gain ? occupancy(k_e_batch<T, 4, false, true>, 128, L::SMEM)
+                    : occupancy(k_e_batch<T, 4, false, false>, 128, L::SMEM);
+    }
+    using L = StageLayout<T, 8>;
+    if (!eside) return pml ? occupancy(k_h_batch<T, 8, true>, 256, L::SMEM)
+                           : occupancy(k_h_batch<T, 8, false>, 256, L::SMEM);
+    if (pml) return gain ? occupancy(k_e_batch<T, 8, true, true>, 256, L::SMEM)
+                         : occupancy(k_e_batch<T, 8, true, false>, 256, L::SMEM);
+    return gain ? occupancy(k_e_batch<T, 8, false, true>, 256, L::SMEM)
+                : occupancy(k_e_batch<T, 8, false, false>, 256, L::SMEM);
+}
+
+template <typename T>
+void batch_kernel_attributes()
+{
+    smem_attr<k_h_batch<T, 4, false>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_h_batch<T, 4, true>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_h_batch<T, 8, false>>(StageLayout<T, 8>::SMEM);
+    smem_attr<k_h_batch<T, 8, true>>(StageLayout<T, 8>::SMEM);
+    smem_attr<k_e_batch<T, 4, false, false>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_e_batch<T, 4, false, true>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_e_batch<T, 4, true, false>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_e_batch<T, 4, true, true>>(StageLayout<T, 4>::SMEM);
+    smem_attr<k_e_batch<T, 8, false, false>>(StageLayout<T, 8>::SMEM);
+    smem_attr<k_e_batch<T, 8, false, true>>(StageLayout<T, 8>::SMEM);
+    smem_attr<k_e_batch<T, 8, true, false>>(StageLayout<T, 8>::SMEM);
+    smem_attr<k_e_batch<T, 8, true, true>>(StageLayout<T, 8>::SMEM);
+    dft_batch_attributes<T>();
+}
+
+#define CPS_BATCH_INSTANTIATE(T)                                                                             \
+    template void launch_h_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, bool, int *,          \
+                                    cudaStream_t);                                                           \
+    template void launch_e_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, bool, bool, int *,   \
+                                    cudaStream_t);                                                           \
+    template void launch_dl_batch<T>(const BatchGrid<T> *, const int4 *, int, cudaStream_t);                 \
+    template void launch_advance_batch<T>(BatchGrid<T> *, int, int, cudaStream_t);                           \
+    template int batch_blocks_per_sm<T>(int, bool, bool, bool);                                              \
+    template void batch_kernel_attributes<T>();
+CPS_BATCH_INSTANTIATE(float)
+CPS_BATCH_INSTANTIATE(double)
+
+}  // namespace cps

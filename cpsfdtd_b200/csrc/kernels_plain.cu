@@ -4,6 +4,7 @@
 // the reference's order, so the FP64 instantiation reproduces the reference
 // arithmetic of BasicFDTD.cpp, CPML.cpp, TF_SF.cpp and the oracle's
 // Drude-Lorentz/gain recursions operation by operation.
+#include "batch.h"
 #include "cells.cuh"
 
 namespace cps {
@@ -212,13 +213,11 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
 // TF/SF (and any other table-driven) injection in CSR form: each thread owns
 // one (cell, component) target and adds its contributions in order,
 // F += coef * inc(n - delay) * profile (TF_SF.cpp:992-1087, 1206-1299)
+// one TF/SF target: its contributions in the reference's face order
 template <typename T>
-__global__ void k_inject(FieldView<T> f, const InjTarget *tg, int ntarget, const InjContrib *ct,
-                         const T *table, int Nt, double n, uint32_t face_mask)
+__device__ __forceinline__ void inject_target(const FieldView<T> &f, const InjTarget &q, const InjContrib *ct,
+                                              const T *table, int Nt, double n, uint32_t face_mask)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntarget) return;
-    const InjTarget q = tg[t];
     T *F[6] = {f.Ex, f.Ey, f.Ez, f.Hx, f.Hy, f.Hz};
     T v = F[q.comp][q.idx];
     for (int c = q.start; c < q.start + q.count; ++c) {
@@ -228,6 +227,45 @@ __global__ void k_inject(FieldView<T> f, const InjTarget *tg, int ntarget, const
         v = v + (T)a.coef * inc * (T)a.profile;
     }
     F[q.comp][q.idx] = v;
+}
+
+template <typename T>
+__global__ void k_inject(FieldView<T> f, const InjTarget *tg, int ntarget, const InjContrib *ct,
+                         const T *table, int Nt, double n, uint32_t face_mask)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntarget) return;
+    inject_target<T>(f, tg[t], ct, table, Nt, n, face_mask);
+}
+
+// batched forms: the step number is the grid's chunk start plus step_off
+template <typename T>
+__global__ void k_inject_batch(const BatchGrid<T> *__restrict__ grids, const int4 *__restrict__ blocks, int side,
+                               int step_off)
+{
+    const int4 e = blocks[blockIdx.x];
+    const int t = e.y + (int)threadIdx.x;
+    if (t >= e.z) return;
+    const BatchGrid<T> &B = grids[e.x];
+    inject_target<T>(B.f, B.tg[side][t], B.ct[side], B.inc[side], B.Nt, (double)(B.n0 + step_off), CPS_FACE_ALL);
+}
+
+template <typename T>
+__global__ void k_sources_batch(const BatchGrid<T> *__restrict__ grids, const int2 *__restrict__ ents, int n,
+                                int step_off)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int2 e = ents[q];
+    const BatchGrid<T> &B = grids[e.x];
+    const int s = e.y;
+    const int64_t nn = B.n0 + step_off;
+    if (nn < 0 || nn >= B.src_len[s]) return;
+    const FieldView<T> &f = B.f;
+    T *F[6] = {f.Ex, f.Ey, f.Ez, f.Hx, f.Hy, f.Hz};
+    const int64_t g = B.src_idx[s];
+    T *dst = F[B.src_comp[s]];
+    dst[g] = dst[g] + (T)B.src_wave[B.src_off[s] + nn];
 }
 
 template <typename T>
@@ -323,6 +361,21 @@ void launch_sources(const FieldView<T> &f, int nsrc, const int64_t *idx, const i
     k_sources<T><<<cdiv(nsrc, 64), 64, 0, s>>>(f, nsrc, idx, comp, waves, wave_off, wave_len, n);
 }
 
+template <typename T>
+void launch_inject_batch(const BatchGrid<T> *grids, const int4 *blocks, int nblocks, int side, int step_off,
+                         cudaStream_t s)
+{
+    if (nblocks <= 0) return;
+    k_inject_batch<T><<<nblocks, 128, 0, s>>>(grids, blocks, side, step_off);
+}
+
+template <typename T>
+void launch_sources_batch(const BatchGrid<T> *grids, const int2 *ents, int n, int step_off, cudaStream_t s)
+{
+    if (n <= 0) return;
+    k_sources_batch<T><<<cdiv(n, 64), 64, 0, s>>>(grids, ents, n, step_off);
+}
+
 #define CPS_INSTANTIATE(T)                                                                              \
     template void launch_h_bulk<T>(const FieldView<T> &, cudaStream_t);                                 \
     template void launch_e_bulk<T>(const FieldView<T> &, cudaStream_t);                                 \
@@ -333,7 +386,9 @@ void launch_sources(const FieldView<T> &f, int nsrc, const int64_t *idx, const i
     template void launch_inject<T>(const FieldView<T> &, const InjTarget *, int, const InjContrib *,    \
                                    const T *, int, double, uint32_t, cudaStream_t);                     \
     template void launch_sources<T>(const FieldView<T> &, int, const int64_t *, const int32_t *,        \
-                                    const double *, const int32_t *, const int32_t *, int, cudaStream_t);
+                                    const double *, const int32_t *, const int32_t *, int, cudaStream_t); \
+    template void launch_inject_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, cudaStream_t); \
+    template void launch_sources_batch<T>(const BatchGrid<T> *, const int2 *, int, int, cudaStream_t);
 CPS_INSTANTIATE(double)
 CPS_INSTANTIATE(float)
 

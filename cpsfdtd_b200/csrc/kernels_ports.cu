@@ -1,13 +1,16 @@
 // kernels_ports.cu -- port sampling, the blocked FP64 port DFT, flux
 // reduction, a non-finite watchdog and host<->device layout conversion.
 //
-// Port samples of every step are gathered into a ring of T slots
-// ([slot][component][point], float on FP32 grids).  Every T steps (and before
-// a read-out) one contraction folds the ring into FP64 accumulators:
-//   acc[c][f][p] += sum_t s[t][c][p] * exp(-i w_f t_c(n_t))
-// with t_c = n dt for E and (n - 1/2) dt for H, i.e. a [P x T] by [T x F]
-// complex product per component, accumulated in FP64.  The phasors of the
-// block are tabulated once per flush into a small scratch table.
+// Port samples of every step are gathered into a ring of slots
+// ([slot][component][point], float on FP32 grids).  Every 64 steps (and
+// before a read-out) one contraction folds the ring into FP64 accumulators,
+//   acc[c][f][p] += s[t][c][p] * exp(-i w_f t_c(n_t))   for t in slot order,
+// with t_c = n dt for E and (n - 1/2) dt for H: a [P x T] by [T x F] complex
+// product per component in which every sample is added to the accumulators
+// on its own, in FP64, so the sums do not depend on how samples are grouped
+// into flushes.  The FP64 phasors of a flush are tabulated once into a
+// scratch table [2][slots][nfreq] (E time, then H time).
+#include "batch.h"
 #include "cells.cuh"
 
 namespace cps {
@@ -32,47 +35,46 @@ __global__ void k_gather(FieldView<T> f, GatherBatch b)
     slot[5 * (int64_t)npts + p] = f.Hz[g];
 }
 
-template <typename R> struct Vec2;
-template <> struct Vec2<float> { using type = float2; };
-template <> struct Vec2<double> { using type = double2; };
+// phasor table of a flush: tab[0][t][f] = (cos, sin)(w_f n_t dt) and
+// tab[1][t][f] = (cos, sin)(w_f (n_t - 1/2) dt), n_t = n_first + t, phases
+// formed as w * (n dt) the way the FP64 oracle forms them; cap = slots of
+// each half
+__device__ __forceinline__ void phasor_entry(const double *omega, int nfreq, int cap, int64_t n_first, double dt,
+                                             int q, double2 *tab)
+{
+    const int t = q / nfreq, fi = q - t * nfreq;
+    const double n = (double)(n_first + t);
+    double s, c;
+    sincos(omega[fi] * (n * dt), &s, &c);
+    tab[q] = make_double2(c, s);
+    sincos(omega[fi] * ((n - 0.5) * dt), &s, &c);
+    tab[(int64_t)cap * nfreq + q] = make_double2(c, s);
+}
 
-// phasor table [t][f] = (cos, sin)(w_f * n_t * dt), phases in FP64, stored in
-// the contraction precision R
-template <typename R>
-__global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_first, double dt,
-                          typename Vec2<R>::type *tab)
+__global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_first, double dt, double2 *tab)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nslots * nfreq) return;
-    const int t = q / nfreq, fi = q - t * nfreq;
-    double s, c;
-    sincos(omega[fi] * ((double)(n_first + t) * dt), &s, &c);
-    tab[q].x = (R)c;
-    tab[q].y = (R)s;
+    phasor_entry(omega, nfreq, nslots, n_first, dt, q, tab);
 }
 
-// Register-tiled contraction: a block of 256 threads covers 64 points x 64
-// frequencies of one component; thread (tp, tf) accumulates points
-// p0 + 16a + tp (a = 0..3) at frequencies f0 + 4tf + b (b = 0..3), so
-// neighbouring lanes touch neighbouring points in shared memory and in the
-// FP64 accumulators.  The block's samples [slots][64] and phasors
-// [slots][64] are staged in shared memory.  Products and the sum over the
-// (at most 64) slots of one flush run in the sample precision T; the block
-// sums are then added to the FP64 accumulators, H components rotated by
-// exp(+i w dt/2) (they sit half a step earlier).
+// Contraction of one flush: a block of 256 threads covers 64 points x 64
+// frequencies of one component; thread (tp, tf) owns points p0 + 16a + tp
+// (a = 0..3) at frequencies f0 + 4tf + b (b = 0..3), so neighbouring lanes
+// touch neighbouring points in shared memory and in the accumulators.  The
+// block's samples [slots][64] and phasors [slots][64] are staged in shared
+// memory; each thread loads its 16 FP64 accumulator pairs, adds the samples
+// one slot at a time (acc_re += s cos, acc_im -= s sin, FP64 fused
+// multiply-adds) and stores them back.
 constexpr int kPT = 64, kFT = 64, kMaxSlots = 64;
+constexpr size_t kDftSmem(size_t esz) { return (esz * kPT + sizeof(double2) * kFT) * kMaxSlots; }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots,
-                                             const typename Vec2<T>::type *tab, const double *omega,
-                                             int nfreq, double dt, const int32_t *comps, double *acc)
+__device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
+                                          int comp, int ci, int p0, int f0, double *acc, unsigned char *sh_raw)
 {
-    using V = typename Vec2<T>::type;
-    extern __shared__ __align__(16) unsigned char sh_raw[];
-    T *ss = reinterpret_cast<T *>(sh_raw);                                // [nslots][kPT]
-    V *sp = reinterpret_cast<V *>(sh_raw + sizeof(T) * kMaxSlots * kPT);  // [nslots][kFT]
-    const int ci = blockIdx.y, p0 = blockIdx.x * kPT, f0 = blockIdx.z * kFT;
-    const int comp = comps[ci];
+    T *ss = reinterpret_cast<T *>(sh_raw);                                          // [nslots][kPT]
+    double2 *sp = reinterpret_cast<double2 *>(sh_raw + sizeof(T) * kMaxSlots * kPT);  // [nslots][kFT]
     const int tid = threadIdx.x, tp = tid & 15, tf = tid >> 4;
     for (int q = tid; q < nslots * kPT; q += blockDim.x) {
         const int t = q / kPT, pl = q - t * kPT, p = p0 + pl;
@@ -80,27 +82,33 @@ __global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots
     }
     for (int q = tid; q < nslots * kFT; q += blockDim.x) {
         const int t = q / kFT, fl = q - t * kFT, f = f0 + fl;
-        V z;
-        z.x = T(0); z.y = T(0);
-        sp[q] = f < nfreq ? tab[(int64_t)t * nfreq + f] : z;
+        sp[q] = f < nfreq ? tab[(int64_t)t * nfreq + f] : make_double2(0.0, 0.0);
+    }
+    double re[4][4], im[4][4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const int f = f0 + tf * 4 + b;
+        const double *ar = acc + ((int64_t)(ci * nfreq + min(f, nfreq - 1)) * 2) * npts;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int p = p0 + a * 16 + tp;
+            const bool ok = f < nfreq && p < npts;
+            re[a][b] = ok ? ar[p] : 0.0;
+            im[a][b] = ok ? ar[npts + p] : 0.0;
+        }
     }
     __syncthreads();
-    T re[4][4], im[4][4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) { re[a][b] = T(0); im[a][b] = T(0); }
     for (int t = 0; t < nslots; ++t) {
-        T sv[4];
+        double sv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) sv[a] = ss[t * kPT + a * 16 + tp];
+        for (int a = 0; a < 4; ++a) sv[a] = (double)ss[t * kPT + a * 16 + tp];
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const V w = sp[t * kFT + tf * 4 + b];
+            const double2 w = sp[t * kFT + tf * 4 + b];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
-                re[a][b] = fma(sv[a], w.x, re[a][b]);
-                im[a][b] = fma(-sv[a], w.y, im[a][b]);
+                re[a][b] = __fma_rn(sv[a], w.x, re[a][b]);
+                im[a][b] = __fma_rn(-sv[a], w.y, im[a][b]);
             }
         }
     }
@@ -108,19 +116,70 @@ __global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots
     for (int b = 0; b < 4; ++b) {
         const int f = f0 + tf * 4 + b;
         if (f >= nfreq) continue;
-        double cs = 1.0, sn = 0.0;
-        if (comp >= 3) sincos(omega[f] * (0.5 * dt), &sn, &cs);
         double *ar = acc + ((int64_t)(ci * nfreq + f) * 2) * npts;
-        double *ai = ar + npts;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int p = p0 + a * 16 + tp;
             if (p >= npts) continue;
-            const double r = (double)re[a][b], m = (double)im[a][b];
-            ar[p] += r * cs - m * sn;
-            ai[p] += r * sn + m * cs;
+            ar[p] = re[a][b];
+            ar[npts + p] = im[a][b];
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
+                                             const int32_t *comps, double *acc)
+{
+    extern __shared__ __align__(16) unsigned char sh_raw[];
+    const int ci = blockIdx.y, comp = comps[ci];
+    dft_block<T>(ring, npts, nslots, tab + (comp >= 3 ? (int64_t)nslots * nfreq : 0), nfreq, comp, ci,
+                 blockIdx.x * kPT, blockIdx.z * kFT, acc, sh_raw);
+}
+
+// batched forms over the ports of many grids
+template <typename T>
+__global__ void k_gather_batch(const BatchGrid<T> *__restrict__ grids, const BatchPort<T> *__restrict__ ports,
+                               const int2 *__restrict__ blocks, int step_off)
+{
+    const int2 e = blocks[blockIdx.x];
+    const BatchPort<T> &P = ports[e.x];
+    const int p = e.y + (int)threadIdx.x;
+    const int npts = P.npts;
+    if (p >= npts) return;
+    const FieldView<T> &f = grids[P.grid].f;
+    T *slot = P.ring + (int64_t)(P.slots == 1 ? 0 : step_off) * 6 * npts;
+    const int64_t g = P.idx[p];
+    slot[p] = f.Ex[g];
+    slot[npts + p] = f.Ey[g];
+    slot[2 * (int64_t)npts + p] = f.Ez[g];
+    slot[3 * (int64_t)npts + p] = f.Hx[g];
+    slot[4 * (int64_t)npts + p] = f.Hy[g];
+    slot[5 * (int64_t)npts + p] = f.Hz[g];
+}
+
+template <typename T>
+__global__ void k_phasors_batch(const BatchGrid<T> *__restrict__ grids, const BatchPort<T> *__restrict__ ports,
+                                const int2 *__restrict__ blocks, int nslots)
+{
+    const int2 e = blocks[blockIdx.x];
+    const BatchPort<T> &P = ports[e.x];
+    const int q = e.y + (int)threadIdx.x;
+    if (q >= nslots * P.nfreq) return;
+    const BatchGrid<T> &B = grids[P.grid];
+    phasor_entry(P.omega, P.nfreq, kMaxRing, B.n0, B.dt, q, P.tab);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_dft_batch(const BatchPort<T> *__restrict__ ports,
+                                                   const int4 *__restrict__ blocks, int nslots)
+{
+    extern __shared__ __align__(16) unsigned char sh_raw[];
+    const int4 e = blocks[blockIdx.x];
+    const BatchPort<T> &P = ports[e.x];
+    const int comp = P.comps[e.z];
+    dft_block<T>(P.ring, P.npts, nslots, P.tab + (comp >= 3 ? (int64_t)kMaxRing * P.nfreq : 0), P.nfreq, comp, e.z,
+                 e.y * kPT, e.w * kFT, P.acc, sh_raw);
 }
 
 // flux[f] = 0.5 * Re sum_p (A_p conj(B_p) - C_p conj(D_p)) * dA over the
@@ -198,17 +257,43 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
                      cudaStream_t s)
 {
     if (npts <= 0 || nslots <= 0 || nfreq <= 0 || ncomp <= 0) return;
-    using V = typename Vec2<T>::type;
-    V *tab = reinterpret_cast<V *>(scratch_phasor);
-    k_phasors<T><<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, tab);
+    double2 *tab = reinterpret_cast<double2 *>(scratch_phasor);
+    k_phasors<<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, tab);
     dim3 grid(cdiv(npts, kPT), ncomp, cdiv(nfreq, kFT));
-    const size_t smem = (sizeof(T) * kPT + sizeof(V) * kFT) * kMaxSlots;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_dft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_dft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem(sizeof(T)));
         attr = true;
     }
-    k_dft<T><<<grid, 256, smem, s>>>(ring, npts, nslots, tab, omega, nfreq, dt, comps, acc);
+    k_dft<T><<<grid, 256, kDftSmem(sizeof(T)), s>>>(ring, npts, nslots, tab, nfreq, comps, acc);
+}
+
+template <typename T>
+void launch_gather_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *blocks, int nblocks,
+                         int step_off, cudaStream_t s)
+{
+    if (nblocks <= 0) return;
+    k_gather_batch<T><<<nblocks, 256, 0, s>>>(grids, ports, blocks, step_off);
+}
+
+template <typename T>
+void dft_batch_attributes()
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_dft_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem(sizeof(T)));
+        attr = true;
+    }
+}
+
+template <typename T>
+void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
+                      const int4 *blocks, int nblocks, int nslots, cudaStream_t s)
+{
+    if (nph <= 0 || nblocks <= 0 || nslots <= 0) return;
+    k_phasors_batch<T><<<nph, 256, 0, s>>>(grids, ports, ph_blocks, nslots);
+    dft_batch_attributes<T>();
+    k_dft_batch<T><<<nblocks, 256, kDftSmem(sizeof(T)), s>>>(ports, blocks, nslots);
 }
 
 void launch_port_flux(const double *acc, int npts, int nfreq, int ncomp, const int32_t *sel, double dA,
@@ -245,7 +330,12 @@ void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s
                                      const int32_t *, int, double *, double *, cudaStream_t);              \
     template void launch_count_nonfinite<T>(const FieldView<T> &, unsigned long long *, cudaStream_t);     \
     template void launch_to_device_layout<T>(const double *, T *, Dims, cudaStream_t);                     \
-    template void launch_from_device_layout<T>(const T *, double *, Dims, cudaStream_t);
+    template void launch_from_device_layout<T>(const T *, double *, Dims, cudaStream_t);                   \
+    template void launch_gather_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int, int, \
+                                         cudaStream_t);                                                    \
+    template void launch_dft_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int,       \
+                                      const int4 *, int, int, cudaStream_t);                             \
+    template void dft_batch_attributes<T>();
 CPS_INST(double)
 CPS_INST(float)
 

@@ -312,14 +312,18 @@ def _tangential_mask(axis: str) -> int:
     return m
 
 
-def jittered_lattice(n: int, pitch: float, jitter: float, seed: int):
-    """Centres (cells) of a simple-cubic lattice filling [0,n)^3, jittered by
-    U[-jitter, jitter] per axis from a PCG64 stream."""
+def jittered_lattice(n, pitch: float, jitter: float, seed: int):
+    """Centres (cells) of a simple-cubic lattice filling [0,n)^3 (or a box
+    n = (nx, ny, nz)), jittered by U[-jitter, jitter] per axis from a PCG64
+    stream."""
     rng = np.random.Generator(np.random.PCG64(seed))
-    m = int(n // pitch)
-    off = (n - (m - 1) * pitch) / 2.0
-    base = off + pitch * np.arange(m)
-    cx, cy, cz = np.meshgrid(base, base, base, indexing="ij")
+    dims = (n, n, n) if np.isscalar(n) else tuple(n)
+    axes = []
+    for m_ in dims:
+        m = max(1, int(m_ // pitch))
+        off = (m_ - (m - 1) * pitch) / 2.0
+        axes.append(off + pitch * np.arange(m))
+    cx, cy, cz = np.meshgrid(*axes, indexing="ij")
     cen = np.stack([cx.ravel(), cy.ravel(), cz.ravel()], axis=1)
     return cen + rng.uniform(-jitter, jitter, size=cen.shape)
 
@@ -352,6 +356,41 @@ def config3(n: int = 384, steps: int = 20000, seed: int = 0, nfreq: int = 0,
                              dft_freqs=(np.linspace(0.9, 1.1, nfreq) * C0 / 600e-9) if nfreq else None))
     dk.nsteps = steps
     return dk
+
+
+def config4_member(nx: int, ny: int, nz: int, seed: int, steps: int = 5000, nfreq: int = 32,
+                   npml: int = 8, port: bool = True) -> Deck:
+    """One realization of the disordered-crystal ensemble: the materials and
+    gain of config3 (spheres eps 11.9 r 8 pitch 30 jittered +-4 from `seed` in
+    a gain-doped eps 2.25 background) in an nx x ny x nz box, CPML npml, Ez
+    seed pulse at the centre, spherical port of radius min(n)/2 - npml - 3
+    cells with an FP64 DFT at nfreq frequencies around 600 nm."""
+    d = 10e-9
+    dk = Deck(nx, ny, nz, d, d, d, name=f"c4_{seed}")
+    dk.media = [(1.0, 1.0, 0.0, 0.0), (1.0, 1.0, 0.0, 0.0), (1.0, 1.0, 0.0, 0.0),
+                (11.9, 1.0, 0.0, 0.0), (1.0, 1.0, 0.0, 0.0), (2.25, 1.0, 0.0, 0.0)]
+    cen = jittered_lattice((nx, ny, nz), 30.0, 4.0, seed)
+    dk.ids = rasterize_spheres(dk.shape3, dk.dx, cen, 8.0, 3, background=ID_GAIN)
+    dk.pml = pml_params(npml)
+    dk.gain = gain_params_laser()
+    c = (nx // 2, ny // 2, nz // 2)
+    wave = gaussian_sine(steps + dk.n0 + 1, dk.dt, 600e-9, 5e-15, 15e-15)
+    dk.sources = [(COMP["Ez"], c[0], c[1], c[2], wave)]
+    r = min(nx, ny, nz) / 2.0 - npml - 3
+    if port and r >= 3:
+        dk.ports.append(Port("spherical", dict(r=r * d, xc=(c[0] + 0.5) * d, yc=(c[1] + 0.5) * d,
+                                               zc=(c[2] + 0.5) * d, theta1=0.0, theta2=180.0, phi1=0.0,
+                                               phi2=360.0),
+                             dft_freqs=(np.linspace(0.9, 1.1, nfreq) * C0 / 600e-9) if nfreq else None))
+    dk.nsteps = steps
+    return dk
+
+
+def config4_shapes(count: int = 256, seed: int = 0, edges=(64, 80, 96, 112, 128)):
+    """Box shapes of the ensemble: each axis drawn uniformly from `edges`
+    (PCG64 stream from `seed`), so anisotropic mixes such as 128x64x96 occur."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [tuple(int(v) for v in rng.choice(edges, size=3)) for _ in range(count)]
 
 
 def rasterize_spheres(shape3, d: float, centres, radius: float, mat: int, background: int = 0) -> np.ndarray:

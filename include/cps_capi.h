@@ -271,6 +271,43 @@ CPS_API cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *
 CPS_API cps_status cps_grid_set_sweep(cps_grid *g, int32_t mode);
 CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sweep_ms, int64_t *samples);
 
+/* ---- batched engine (no reference counterpart: main.cpp runs one grid per
+ * process).  A batch advances many independent grids of one precision
+ * together: one launch per sweep class over a table of tiles of all member
+ * grids, then one launch each for the Drude-Lorentz cells, TF/SF injection,
+ * sources and port sampling of all grids; steps run in chunks of at most 64
+ * that end with one port-DFT contraction and are captured into CUDA graphs.
+ * Members are built and read with the one-grid calls above; results are the
+ * same as stepping each grid alone with CPS_PATH_FUSED.  A member changed
+ * between batch steps (set-up calls, cps_step, cps_grid_set_step) is picked
+ * up by the next cps_batch_step.  Grids need nx >= 32, ny >= 8, nz >= 2. */
+typedef struct cps_batch cps_batch;
+CPS_API cps_status cps_batch_create(int32_t precision, cps_batch **out);
+CPS_API cps_status cps_batch_destroy(cps_batch *b);
+CPS_API cps_status cps_batch_add(cps_batch *b, cps_grid *g);
+CPS_API cps_status cps_batch_remove(cps_batch *b, cps_grid *g);
+CPS_API cps_status cps_batch_info(const cps_batch *b, int32_t *ngrids, int64_t *cells);
+/* advance every member by nsteps (asynchronous on the batch stream; member
+ * streams are ordered after it) */
+CPS_API cps_status cps_batch_step(cps_batch *b, int32_t nsteps);
+/* wait for the batch stream; reports a device-side wait that gave up */
+CPS_API cps_status cps_batch_synchronize(cps_batch *b);
+/* tile rows (4 or 8), planes per tile, persistent launch (0: one block per
+ * tile, 1: as many blocks as fit on the device, each walking the table) */
+CPS_API cps_status cps_batch_set_tile(cps_batch *b, int32_t rows, int32_t planes, int32_t persistent);
+CPS_API cps_status cps_batch_get_tile(const cps_batch *b, int32_t *rows, int32_t *planes, int32_t *persistent);
+/* CUDA-graph replay of step chunks (default on) */
+CPS_API cps_status cps_batch_set_graph(cps_batch *b, int32_t on);
+CPS_API cps_status cps_batch_get_stream(const cps_batch *b, void **stream);
+CPS_API cps_status cps_batch_launch_count(const cps_batch *b, int64_t *launches);
+/* autotuner key of the batch: precision, shape bucket and material mix */
+CPS_API cps_status cps_batch_tune_key(const cps_batch *b, char *buf, int32_t len);
+/* choose tile rows, planes and persistence: from cache_path when it holds
+ * the batch's key, else by timing each candidate over trial_steps live steps
+ * (members advance; *steps_run says by how much) and appending the winner */
+CPS_API cps_status cps_batch_autotune(cps_batch *b, const char *cache_path, int32_t trial_steps,
+                                      int32_t *steps_run);
+
 #ifdef __cplusplus
 }
 #endif
