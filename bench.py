@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=2, help="end-to-end jobs to time")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-steps", type=int, default=3, help="time steps in the CPU baseline sample")
+    ap.add_argument("--ens-grids", type=int, default=256, help="grids of the batched ensemble leg (0: skip)")
+    ap.add_argument("--ens-steps", type=int, default=128, help="timed steps of the batched ensemble")
+    ap.add_argument("--ens-loop-steps", type=int, default=8,
+                    help="steps per grid of the one-grid-per-launch comparison loops")
     return ap.parse_args()
 
 
@@ -210,6 +214,80 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ensemble(args, local, dist):
+    """Batched ensemble: --ens-grids disordered-crystal realizations (edges
+    drawn from {64,80,96,112,128} per axis, CPML 8, gain, 32-frequency
+    spherical-port DFT) advanced together by the batched engine (autotuned
+    tiling, graph-replayed 64-step chunks), against the same grids stepped one
+    grid per launch, one after another, on the plain per-routine path and on
+    the fused path."""
+    import torch
+    import cpsfdtd_b200 as cps
+    from cpsfdtd_b200 import decks
+    t0 = time.perf_counter()
+    shapes = decks.config4_shapes(args.ens_grids, seed=0)
+    grids = []
+    for i, (nx, ny, nz) in enumerate(shapes):
+        dk = decks.config4_member(nx, ny, nz, seed=i, steps=5000, nfreq=32)
+        grids.append(cps.Grid.from_deck(dk, cps.FP32, device=local))
+    setup_s = time.perf_counter() - t0
+    cells = sum(nx * ny * nz for nx, ny, nz in shapes)
+    b = cps.Batch(cps.FP32)
+    for g in grids:
+        b.add(g)
+    cache = os.path.join(os.path.expanduser("~"), ".cache", "cpsfdtd_b200", "batch_tune.txt")
+    os.makedirs(os.path.dirname(cache), exist_ok=True)
+    t1 = time.perf_counter()
+    tuned_steps = b.autotune(cache, trial_steps=4)
+    tune_s = time.perf_counter() - t1
+    b.step(64)  # warm-up chunk (graph capture)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream(), device=local)
+    l0 = b.launches()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.ens_steps)
+    e1.record(stream)
+    b.sync()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    batched = cells * args.ens_steps / (ms / 1e3) / 1e9
+    launches = b.launches() - l0
+    tile = list(b.get_tile())
+    b.close()
+
+    def loop(path):
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        for g in grids:
+            g.step(args.ens_loop_steps, path)
+            g.sync()
+        torch.cuda.synchronize()
+        return cells * args.ens_loop_steps / (time.perf_counter() - ts) / 1e9
+
+    loop(cps.FUSED)  # warm-up of the one-grid kernels
+    plain = loop(cps.PLAIN)
+    fused = loop(cps.FUSED)
+    for g in grids:
+        g.close()
+    return {"workload": f"{args.ens_grids} disordered-crystal realizations, edges U{{64,80,96,112,128}} per axis, "
+                        "CPML 8, four-level gain, Ez seed pulse, 32-freq FP64 spherical-port DFT; FP32 fields",
+            "grids": args.ens_grids, "cells": int(cells), "metric": "Gcell-upd/s", "value": batched,
+            "steps_timed": args.ens_steps, "ms": ms, "tile": tile,
+            "plain_one_grid_per_launch": plain, "fused_one_grid_per_launch": fused,
+            "speedup_vs_plain_loop": batched / plain if plain else None,
+            "speedup_vs_fused_loop": batched / fused if fused else None,
+            "gpu_launches": int(launches), "setup_s": setup_s, "autotune_s": tune_s,
+            "autotune_steps": tuned_steps, "loop_steps_per_grid": args.ens_loop_steps,
+            "timing": "batched: CUDA events on the batch stream; loops: host clock with a device sync per grid"}
+
+
 def run_ours(args):
     import torch
     world, rank, local, dist = dist_setup()
@@ -314,6 +392,12 @@ def run_ours(args):
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
+    ens = None
+    if args.ens_grids > 0:
+        try:
+            ens = ensemble(args, local, dist)
+        except Exception as ex:
+            ens = {"error": str(ex)}
     if rank == 0:
         line = {"metric": "Gcell-upd/s", "value": value, "unit": "Gcell-upd/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -326,7 +410,7 @@ def run_ours(args):
                            "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
                            "l2": "inputs larger than L2 (fields 0.40 GB per grid)", "parallelism": f"replicas x{world}"},
                 "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
-                "e2e": e2e, "cpu_baseline": cpu}
+                "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens}
         print(json.dumps(line), flush=True)
     g.close()
     if dist:

@@ -737,6 +737,12 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     G.t32t21dt = p->t32 * p->t21 * dt; G.t32t21_2 = 2.0 * p->t32 * p->t21; G.t32_2 = p->t32 / 2.0;
     G.pump_dt = p->pump_rate * dt;
     G.scaleP = g->fp32 ? G.CEP : 1.0;
+    G.fa1 = (float)G.CPa1; G.fa2 = (float)G.CPa2; G.fa3 = (float)(G.CPa3 * G.scaleP);
+    G.fb1 = (float)G.CPb1; G.fb2 = (float)G.CPb2; G.fb3 = (float)(G.CPb3 * G.scaleP);
+    G.r_t30 = 1.0 / G.t30; G.r_t32 = 1.0 / G.t32; G.r_t21 = 1.0 / G.t21; G.r_t10 = 1.0 / G.t10;
+    G.r_t21_2 = 1.0 / G.t21_2; G.r_t32_2 = 1.0 / G.t32_2;
+    G.r_hwb = 1.0 / G.homega_bdt; G.r_hwa = 1.0 / G.homega_adt;
+    G.inv_scale = 1.0 / G.scaleP;
     g->gain_id = p->gain_id;
     if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg))) return s;
     const int nw = g->fp32 ? kG32Words : kG64Words;

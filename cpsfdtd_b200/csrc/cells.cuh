@@ -88,6 +88,28 @@ __device__ __forceinline__ void gain_p_update(const GainCoef &G, const double N[
     }
 }
 
+// FP32 grids: the same recursion with the float coefficients prepared on the
+// host (bit-identical to converting them here)
+template <>
+__device__ __forceinline__ void gain_p_update<float>(const GainCoef &G, const double N[4], const float E[3],
+                                                     float Pa[3], float Pa1[3], float Pa2[3], float Pb[3],
+                                                     float Pb1[3], float Pb2[3])
+{
+    const float dNa = (float)(N[2] - N[1]), dNb = (float)(N[3] - N[0]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        Pa2[c] = Pa1[c];
+        Pa1[c] = Pa[c];
+        Pa[c] = G.fa1 * Pa[c] + G.fa2 * Pa2[c] + E[c] * G.fa3 * dNa;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        Pb2[c] = Pb1[c];
+        Pb1[c] = Pb[c];
+        Pb[c] = G.fb1 * Pb[c] + G.fb2 * Pb2[c] + E[c] * G.fb3 * dNb;
+    }
+}
+
 // E correction (FourLevelLaser.cpp:302-305): E -= CEP (dPa + dPb)
 template <typename T>
 __device__ __forceinline__ T gain_e_corr(const GainCoef &G, T E, T pa, T pa1, T pb, T pb1)
@@ -122,6 +144,30 @@ __device__ __forceinline__ void gain_n_update(const GainCoef &G, double N[4], co
            (N[1] * ((N[0] - 1) / G.t10 - N[2] / G.t21 + G.dt_2) + N[2] / G.t21_2 - sa / G.homega_adt);
     N[2] = G.t32t21dt / (G.t32t21_2 + G.t21dt * N[3] + G.t32dt * (1 - N[1])) *
            (N[2] * ((N[1] - 1) / G.t21 - N[3] / G.t32 + G.dt_2) + N[3] / G.t32_2 + s2 / G.homega_adt);
+    N[0] = 2.0 - N[1] - N[2] - N[3];
+}
+
+// FP32 grids: the energy-exchange sums E.(P - P'') are formed in float (P
+// carries the factor CEP), the populations stay FP64 with the constant
+// divisors applied as host-computed reciprocals; N0 from conservation in FP64.
+template <>
+__device__ __forceinline__ void gain_n_update<float>(const GainCoef &G, double N[4], const float E[3],
+                                                     const float E1[3], const float Pa[3], const float Pa1[3],
+                                                     const float Pa2[3], const float Pb[3], const float Pb2[3])
+{
+    const float fsb = E1[0] * (Pb[0] - Pb2[0]) + E1[1] * (Pb[1] - Pb2[1]) + E1[2] * (Pb[2] - Pb2[2]);
+    const float fsa = E1[0] * (Pa[0] - Pa2[0]) + E1[1] * (Pa[1] - Pa2[1]) + E1[2] * (Pa[2] - Pa2[2]);
+    const float fs2 = (E[0] + E1[0]) * (Pa[0] - Pa2[0]) + (E[1] + E1[1]) * (Pa[1] - Pa1[1]) +
+                      (E[2] + E1[2]) * (Pa[2] - Pa2[2]);
+    const double sb = (double)fsb * G.inv_scale, sa = (double)fsa * G.inv_scale, s2 = (double)fs2 * G.inv_scale;
+    const double N0old = N[0];
+    N[3] = G.t30t32dt / (G.t30t32_2 + G.t30dt * (1 - N[2]) + G.t32dt * (1 - N[0])) *
+           (N[3] * ((N[0] - 1) * G.r_t30 + (N[2] - 1) * G.r_t32 + G.dt_2) + sb * G.r_hwb);
+    N[3] = N[3] + G.pump_dt * N0old;
+    N[1] = G.t10t21dt / (G.t10t21_2 + G.t10dt * N[2] + G.t21dt * (1 - N[0])) *
+           (N[1] * ((N[0] - 1) * G.r_t10 - N[2] * G.r_t21 + G.dt_2) + N[2] * G.r_t21_2 - sa * G.r_hwa);
+    N[2] = G.t32t21dt / (G.t32t21_2 + G.t21dt * N[3] + G.t32dt * (1 - N[1])) *
+           (N[2] * ((N[1] - 1) * G.r_t21 - N[3] * G.r_t32 + G.dt_2) + N[3] * G.r_t32_2 + s2 * G.r_hwa);
     N[0] = 2.0 - N[1] - N[2] - N[3];
 }
 

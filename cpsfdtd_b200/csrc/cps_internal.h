@@ -66,6 +66,10 @@ struct GainCoef {
     double t32t21dt, t32t21_2, t32_2;
     double pump_dt;
     double scaleP;  // P stored = scaleP * P
+    // FP32 grids: P coefficients in float (CP3 carrying scaleP) and the
+    // constant divisors of the population update as FP64 reciprocals
+    float fa1, fa2, fa3, fb1, fb2, fb3;
+    double r_t30, r_t32, r_t21, r_t10, r_t21_2, r_t32_2, r_hwb, r_hwa, inv_scale;
 };
 
 // per-cell gain state words
