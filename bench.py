@@ -22,6 +22,7 @@ Multi-GPU: one replica job per rank (the path does not shard), weak scaling.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -61,6 +62,11 @@ def parse():
     ap.add_argument("--ens-steps", type=int, default=128, help="timed steps of the batched ensemble")
     ap.add_argument("--ens-loop-steps", type=int, default=8,
                     help="steps per grid of the one-grid-per-launch comparison loops")
+    ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving leg (0: skip)")
+    ap.add_argument("--serve-step-scale", type=float, default=2.0,
+                    help="job step counts are the log-uniform [500, 20000] draws divided by this")
+    ap.add_argument("--serve-load", type=float, default=2.0,
+                    help="offered load: arrival rate x job work / 20 Gcell-upd/s")
     return ap.parse_args()
 
 
@@ -240,7 +246,7 @@ def ensemble(args, local, dist):
     t1 = time.perf_counter()
     tuned_steps = b.autotune(cache, trial_steps=4)
     tune_s = time.perf_counter() - t1
-    b.step(64)  # warm-up chunk (graph capture)
+    b.step(128)  # warm-up: a direct 64-step chunk, then its graph capture and replay
     b.sync()
     stream = torch.cuda.ExternalStream(b.stream(), device=local)
     l0 = b.launches()
@@ -286,6 +292,116 @@ def ensemble(args, local, dist):
             "gpu_launches": int(launches), "setup_s": setup_s, "autotune_s": tune_s,
             "autotune_steps": tuned_steps, "loop_steps_per_grid": args.ens_loop_steps,
             "timing": "batched: CUDA events on the batch stream; loops: host clock with a device sync per grid"}
+
+
+def serve_jobs(count, step_scale, seed=0):
+    """Seeded job stream: edge log-uniform in [48, 320], steps log-uniform in
+    [500, 20000] (divided by step_scale), material mix 40% dielectric (the
+    sphere-scatterer deck), 35% Drude-Lorentz spheres + TF/SF + six 64-frequency
+    planar-port DFTs (dispersive-scattering parameters), 25% four-level gain
+    photonic crystal with a 32-frequency spherical-port DFT (laser parameters)."""
+    from cpsfdtd_b200 import decks
+    rng = np.random.Generator(np.random.PCG64(seed))
+    jobs = []
+    for n in range(count):
+        edge = int(round(math.exp(rng.uniform(math.log(48), math.log(320)))))
+        steps = int(round(math.exp(rng.uniform(math.log(500), math.log(20000))) / step_scale))
+        steps = max(1, steps)
+        u = rng.uniform()
+        kind = "dielectric" if u < 0.40 else ("drude-lorentz" if u < 0.75 else "gain")
+        jobs.append((kind, edge, steps, n))
+    return jobs
+
+
+def serve_deck(kind, edge, steps, seed):
+    from cpsfdtd_b200 import decks
+    if kind == "dielectric":
+        return decks.config1(n=edge, steps=steps)
+    if kind == "drude-lorentz":
+        return decks.config2(n=edge, steps=steps, nfreq=64)
+    return decks.config3(n=edge, steps=steps, seed=seed, nfreq=32)
+
+
+def serving(args, local):
+    """Served job stream through the library's serving loop (Poisson arrivals
+    offered at --serve-load times a 20 Gcell-upd/s service rate, admission
+    against a 180 GB budget, continuous batching), against the same jobs run
+    one at a time on the plain per-routine GPU path, queued in arrival order."""
+    import torch
+    import cpsfdtd_b200 as cps
+    jobs = serve_jobs(args.serve_jobs, args.serve_step_scale)
+    work = [e ** 3 * st for _, e, st, _ in jobs]
+    rng = np.random.Generator(np.random.PCG64(1))
+    mean_gap = sum(work) / (args.serve_load * 20e9) / len(jobs)
+    arrivals = np.cumsum(rng.exponential(mean_gap, size=len(jobs)))
+    arrivals -= arrivals[0]
+    budget = 180 * 10 ** 9
+    free, total = torch.cuda.mem_get_info(local)
+    budget = min(budget, int(free * 0.9))
+    srv = cps.Server(cps.FP32, max_jobs=256, budget_bytes=budget, chunk_steps=64)
+    done = {}
+    t0 = time.perf_counter()
+    nxt = 0
+    while len(done) < len(jobs):
+        now = time.perf_counter() - t0
+        while nxt < len(jobs) and arrivals[nxt] <= now:
+            kind, edge, steps, seed = jobs[nxt]
+            dk = serve_deck(kind, edge, steps, seed)
+
+            def fin(g, status, n=nxt):
+                if g is not None and status == 0:
+                    for p in range(len(g.ports)):
+                        if g.ports[p][2] > 0:
+                            g.port_dft(p, raw=True)
+                done[n] = (status, time.perf_counter() - t0)
+
+            srv.submit(lambda dk=dk: cps.Grid.from_deck(dk, cps.FP32, device=local), fin, steps,
+                       cps.footprint(dk))
+            nxt += 1
+        live, queued = srv.poll()
+        if live == 0 and queued == 0 and nxt < len(jobs):
+            time.sleep(max(0.0, min(0.05, arrivals[nxt] - (time.perf_counter() - t0))))
+    span = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = sorted(done[n][1] - arrivals[n] for n in range(len(jobs)))
+    cells_total = float(sum(work))
+
+    # the same jobs one at a time on the plain path, in arrival order
+    service = []
+    for kind, edge, steps, seed in jobs:
+        dk = serve_deck(kind, edge, steps, seed)
+        torch.cuda.synchronize()
+        ts = time.perf_counter()
+        g = cps.Grid.from_deck(dk, cps.FP32, device=local)
+        g.step(steps, cps.PLAIN)
+        for p in range(len(g.ports)):
+            if g.ports[p][2] > 0:
+                g.port_dft(p, raw=True)
+        g.sync()
+        g.close()
+        service.append(time.perf_counter() - ts)
+    finish, plain_lat = 0.0, []
+    for a, sv in zip(arrivals, service):
+        finish = max(finish, a) + sv
+        plain_lat.append(finish - a)
+    plain_lat.sort()
+    pct = lambda v, q: float(np.percentile(v, q))
+    return {"workload": f"{len(jobs)} jobs, edge log-uniform [48,320], steps log-uniform [500,20000]/"
+                        f"{args.serve_step_scale:g}, mix 40% dielectric / 35% Drude-Lorentz+TF/SF / 25% gain; "
+                        f"Poisson arrivals at {args.serve_load:g}x a 20 Gcell-upd/s service rate; FP32 fields, "
+                        "FP64 port accumulators",
+            "jobs": len(jobs), "jobs_per_s": len(jobs) / span, "gcell_upd_per_s": cells_total / span / 1e9,
+            "latency_p50_s": pct(lat, 50), "latency_p99_s": pct(lat, 99),
+            "server_latency_p50_ms": st["latency_p50_ms"], "server_latency_p99_ms": st["latency_p99_ms"],
+            "wait_p50_ms": st["wait_p50_ms"], "chunks": st["chunks"], "failed": st["jobs_failed"],
+            "budget_bytes": budget, "span_s": span,
+            "plain_one_at_a_time": {"jobs_per_s": len(jobs) / max(finish, 1e-9),
+                                    "gcell_upd_per_s": cells_total / sum(service) / 1e9,
+                                    "latency_p50_s": pct(plain_lat, 50), "latency_p99_s": pct(plain_lat, 99)},
+            "speedup_gcell_vs_plain": (cells_total / span) / (cells_total / sum(service)),
+            "timing": "host clock: job latency = completion - arrival, including deck generation and grid "
+                      "set-up; plain latencies from measured service times queued in arrival order"}
 
 
 def run_ours(args):
@@ -392,6 +508,12 @@ def run_ours(args):
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
+    srv = None
+    if args.serve_jobs > 0 and world == 1:
+        try:
+            srv = serving(args, local)
+        except Exception as ex:
+            srv = {"error": str(ex)}
     ens = None
     if args.ens_grids > 0:
         try:
@@ -410,7 +532,7 @@ def run_ours(args):
                            "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
                            "l2": "inputs larger than L2 (fields 0.40 GB per grid)", "parallelism": f"replicas x{world}"},
                 "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
-                "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens}
+                "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens, "serving": srv}
         print(json.dumps(line), flush=True)
     g.close()
     if dist:

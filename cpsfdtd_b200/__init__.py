@@ -16,9 +16,11 @@ import ctypes as C
 import os
 from typing import Optional
 
+from .decks import ID_DISPERSIVE
+
 import numpy as np
 
-__all__ = ["Grid", "Batch", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
+__all__ = ["Grid", "Batch", "Server", "footprint", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcpsfdtd.so")
@@ -133,6 +135,10 @@ def lib():
             "cps_batch_launch_count": ([P, C.POINTER(I64)], I32),
             "cps_batch_tune_key": ([P, C.c_char_p, I32], I32),
             "cps_batch_autotune": ([P, C.c_char_p, I32, ip], I32),
+            "cps_server_create": ([P, C.POINTER(P)], I32), "cps_server_destroy": ([P], I32),
+            "cps_server_submit": ([P, I64, I32, _BUILD_FN, _DONE_FN, P, C.POINTER(I64)], I32),
+            "cps_server_poll": ([P, ip, ip], I32), "cps_server_drain": ([P], I32),
+            "cps_server_cancel": ([P, I64], I32), "cps_server_get_stats": ([P, P], I32),
         }
         for name, (args, res) in sigs.items():
             fn = getattr(L, name)
@@ -474,3 +480,132 @@ class Batch:
         ran = C.c_int32()
         _check(self.L.cps_batch_autotune(self.h, cache_path.encode(), trial_steps, C.byref(ran)))
         return ran.value
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("max_jobs", C.c_int32), ("budget_bytes", C.c_int64),
+                ("chunk_steps", C.c_int32), ("tile_rows", C.c_int32), ("tile_planes", C.c_int32),
+                ("tile_persistent", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("jobs_done", "jobs_failed", "jobs_rejected", "jobs_cancelled",
+                                          "jobs_live", "jobs_queued", "bytes_in_use", "chunks")] + \
+               [(n, C.c_double) for n in ("latency_p50_ms", "latency_p99_ms", "wait_p50_ms", "wait_p99_ms",
+                                           "run_p50_ms", "cell_updates", "span_s")]
+
+
+_BUILD_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_void_p))
+_DONE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32)
+
+CPS_E_INVALID, CPS_E_BUDGET, CPS_E_CANCELLED = 1, 6, 8
+
+
+def footprint(dk, precision=FP32) -> int:
+    """Admission estimate of a deck's device memory in bytes: fields, IDs,
+    CPML slabs, Drude-Lorentz and gain state at their cell counts, port rings
+    and DFT accumulators, plus 5% for tables."""
+    esz = 4 if precision == FP32 else 8
+    nx, ny, nz = dk.nx, dk.ny, dk.nz
+    px = (nx + 1 + 31) // 32 * 32
+    cells = px * (ny + 1) * (nz + 1)
+    total = 6 * cells * esz + cells
+    if dk.pml:
+        n = dk.pml["npml"]
+        xw = sum((v + 32) // 32 * 32 for v in n[0:2] if v) * (ny + 1) * (nz + 1)
+        yw = sum(v + 1 for v in n[2:4] if v) * px * (nz + 1)
+        zw = sum(v + 1 for v in n[4:6] if v) * px * (ny + 1)
+        total += 2 * 2 * esz * (xw + yw + zw)  # two psi per slab cell for E and for H
+    ids = dk.ids
+    if dk.dl:
+        ndl = int((ids == ID_DISPERSIVE).sum()) if ids is not None else cells // 10
+        total += ndl * (3 * (len(dk.dl.get("fD", [])) + 2 * len(dk.dl.get("fL", [])) + 1) * esz + 8)
+    if dk.gain:
+        gid = dk.gain.get("gain_id", 5)
+        ng = int((ids == gid).sum()) if ids is not None else cells
+        total += ng * ((24 if precision == FP32 else 25) * esz + 8)
+    for p in dk.ports:
+        npts = len(port_points(dk, p))
+        nf = 0 if p.dft_freqs is None else len(p.dft_freqs)
+        nc = bin(p.dft_mask & 63).count("1") if nf else 0
+        total += npts * (8 + 6 * esz * (64 if nf else 1) + nc * nf * 16)
+    return int(total * 1.05)
+
+
+class Server:
+    """Serving loop of the library (``cps_server_*``): jobs queued with a
+    footprint and step count, admitted against a device-memory budget and run
+    together by the batched engine; a job's ``build()`` makes its Grid when it
+    is admitted and ``done(grid, status)`` reads its results when it ends (the
+    server destroys the grid afterwards)."""
+
+    def __init__(self, precision=FP32, max_jobs=64, budget_bytes=180 * 10 ** 9, chunk_steps=64, tile=None):
+        self.L = lib()
+        self.h = C.c_void_p()
+        rows, planes, pers = tile if tile else (0, 0, 0)
+        cfg = ServerConfig(precision, max_jobs, int(budget_bytes), chunk_steps, rows, planes, pers)
+        _check(self.L.cps_server_create(C.byref(cfg), C.byref(self.h)))
+        self._jobs = {}
+        self._grids = {}
+        self.errors = {}
+        self._build_cb = _BUILD_FN(self._on_build)
+        self._done_cb = _DONE_FN(self._on_done)
+
+    def _on_build(self, user, jid, out):
+        try:
+            g = self._jobs[jid][0]()
+        except CpsError as ex:
+            self.errors[jid] = str(ex)
+            return ex.code
+        except Exception as ex:  # a malformed job fails alone
+            self.errors[jid] = repr(ex)
+            return CPS_E_INVALID
+        self._grids[jid] = g
+        out[0] = g.h.value
+        return 0
+
+    def _on_done(self, user, jid, gptr, status):
+        g = self._grids.pop(jid, None)
+        job = self._jobs.pop(jid, None)
+        try:
+            if job is not None and job[1] is not None:
+                job[1](g, status)
+        except Exception as ex:
+            self.errors[jid] = repr(ex)
+        finally:
+            if g is not None:
+                g.h = C.c_void_p()  # the server destroys the grid when this returns
+
+    def submit(self, build, done, nsteps, footprint_bytes):
+        jid = C.c_int64()
+        _check(self.L.cps_server_submit(self.h, int(footprint_bytes), int(nsteps), self._build_cb, self._done_cb,
+                                        None, C.byref(jid)))
+        self._jobs[jid.value] = (build, done)
+        return jid.value
+
+    def poll(self):
+        live, queued = C.c_int32(), C.c_int32()
+        _check(self.L.cps_server_poll(self.h, C.byref(live), C.byref(queued)))
+        return live.value, queued.value
+
+    def drain(self):
+        _check(self.L.cps_server_drain(self.h))
+
+    def cancel(self, jid):
+        _check(self.L.cps_server_cancel(self.h, jid))
+
+    def stats(self):
+        s = ServerStats()
+        _check(self.L.cps_server_get_stats(self.h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.L.cps_server_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -34,6 +34,7 @@ SOURCES = {
     "kernels_ports.cu": [],
     "kernels_batch.cu": [],
     "batch.cpp": ["-x", "cu"],
+    "server.cpp": ["-x", "cu"],
 }
 
 

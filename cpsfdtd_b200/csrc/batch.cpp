@@ -98,6 +98,7 @@ struct cps_batch {
     int64_t cells = 0;
     // graphs per chunk length
     std::map<int, std::pair<cudaGraphExec_t, int64_t>> graphs;  // executable and its kernel count
+    std::map<int, int> direct;  // chunk lengths launched directly since the last rebuild
     std::vector<cudaEvent_t> ev;  // one per member grid (ordering with the grid streams)
     cudaEvent_t done = nullptr;
     int64_t launches = 0;
@@ -109,7 +110,7 @@ cps_status bmalloc(cps_batch *b, void **p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMallocAsync(p, bytes, b->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_error(std::string("batch table allocation of ") + std::to_string(bytes) + " bytes failed");
@@ -132,13 +133,14 @@ void drop_graphs(cps_batch *b)
 {
     for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second.first);
     b->graphs.clear();
+    b->direct.clear();
 }
 
 void free_tables(cps_batch *b)
 {
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
-    for (void *p : b->owned) cudaFree(p);
+    for (void *p : b->owned) cudaFreeAsync(p, b->stream);
     b->owned.clear();
     b->d_grids = b->d_ports = nullptr;
     b->d_err = nullptr;
@@ -352,10 +354,13 @@ int64_t enqueue_chunk(cps_batch *b, int S)
     return n + 1;
 }
 
+// A chunk length is launched directly the first time after a rebuild and
+// captured into a graph when it comes again, so membership that changes every
+// chunk (serving) does not pay for captures it never replays.
 template <typename T>
 cps_status run_chunk(cps_batch *b, int S)
 {
-    if (!b->graph) {
+    if (!b->graph || (b->graphs.find(S) == b->graphs.end() && b->direct[S]++ == 0)) {
         b->launches += enqueue_chunk<T>(b, S);
         cudaError_t e = cudaGetLastError();
         REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("batch launch failed: ") + cudaGetErrorString(e));

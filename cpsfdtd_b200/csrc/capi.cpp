@@ -35,7 +35,9 @@ cps_status dalloc(cps_grid *g, void **p, size_t bytes)
 {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    // stream-ordered pool allocation: freeing a finished job's arrays returns
+    // them to the device pool without a device-wide synchronisation
+    cudaError_t e = cudaMallocAsync(p, bytes, g->stream);
     if (e != cudaSuccess) {
         set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
         cudaGetLastError();
@@ -52,7 +54,7 @@ void dfree(cps_grid *g, void *p)
     if (!p) return;
     for (auto it = g->owned.begin(); it != g->owned.end(); ++it)
         if (it->first == p) { g->owned.erase(it); break; }
-    cudaFree(p);
+    cudaFreeAsync(p, g->stream);
 }
 
 template <typename T>
@@ -170,16 +172,20 @@ cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cel
     return upload_raw(g, *d_seg, seg.data(), seg.size() * sizeof(int32_t));
 }
 
-void gain_initial_state(cps_grid *g, std::vector<double> &words, int64_t n)
+// initial gain state, SoA [word][cell]: all zero (FP32 keeps population
+// offsets) except FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197)
+cps_status gain_state_init(cps_grid *g)
 {
-    // SoA [word][cell]; FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197); FP32 keeps offsets (all 0)
     const int nw = g->fp32 ? kG32Words : kG64Words;
-    words.assign((size_t)nw * n, 0.0);
-    if (!g->fp32)
-        for (int64_t c = 0; c < n; ++c) {
-            words[(size_t)21 * n + c] = 1.0;
-            words[(size_t)22 * n + c] = 1.0;
-        }
+    CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)g->g_n * nw * g->esz, g->stream));
+    if (!g->fp32 && g->g_n > 0) {
+        const std::vector<double> ones((size_t)g->g_n, 1.0);
+        for (int w : {21, 22})  // FP64 layout words of N0 and N1
+            CK(cudaMemcpyAsync((double *)g->d_g_state + (size_t)w * g->g_n, ones.data(), ones.size() * sizeof(double),
+                               cudaMemcpyHostToDevice, g->stream));
+    }
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
 }
 
 cps_status flush_dft(cps_grid *g, PortState &P);
@@ -443,6 +449,22 @@ extern "C" cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out)
     CK(cudaGetDeviceCount(&ndev));
     REQUIRE(desc->device >= 0 && desc->device < ndev, CPS_E_INVALID, "no such CUDA device");
     CK(cudaSetDevice(desc->device));
+    {
+        // this process's default pool on the device keeps freed memory for the
+        // next grid instead of handing it back to the driver
+        static std::mutex pool_mu;
+        static std::vector<int> pooled;
+        std::lock_guard<std::mutex> lk(pool_mu);
+        if (std::find(pooled.begin(), pooled.end(), desc->device) == pooled.end()) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, desc->device) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            cudaGetLastError();
+            pooled.push_back(desc->device);
+        }
+    }
     cps_grid *g = new cps_grid();
     g->desc = *desc;
     if (!(g->desc.dt > 0)) g->desc.dt = cps_courant_dt(desc->dx, desc->dy, desc->dz);
@@ -481,9 +503,9 @@ extern "C" cps_status cps_grid_destroy(cps_grid *g)
 {
     if (!g) return CPS_OK;
     cudaSetDevice(g->desc.device);
-    if (g->stream) cudaStreamSynchronize(g->stream);
-    for (auto &a : g->owned) cudaFree(a.first);
+    for (auto &a : g->owned) cudaFreeAsync(a.first, g->stream);
     g->owned.clear();
+    if (g->stream) cudaStreamSynchronize(g->stream);
     for (auto &e : g->ev) cudaEventDestroy(e);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     delete g;
@@ -747,9 +769,7 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg))) return s;
     const int nw = g->fp32 ? kG32Words : kG64Words;
     if ((s = dalloc(g, &g->d_g_state, (size_t)g->g_n * nw * g->esz))) return s;
-    std::vector<double> init;
-    gain_initial_state(g, init, g->g_n);
-    if ((s = upload_real(g, g->d_g_state, init.data(), init.size()))) return s;
+    if ((s = gain_state_init(g))) return s;
     g->gain_on = true;
     return CPS_OK;
 }
@@ -825,9 +845,12 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
     const int compE[3][2] = {{CPS_EY, CPS_EZ}, {CPS_EX, CPS_EZ}, {CPS_EX, CPS_EY}};
     const int compH[3][2] = {{CPS_HZ, CPS_HY}, {CPS_HZ, CPS_HX}, {CPS_HY, CPS_HX}};
     const int order[6] = {kFY1, kFY2, kFX1, kFX2, kFZ1, kFZ2};
+    struct Item {
+        int64_t key;  // idx * 8 + comp
+        InjContrib c;
+    };
     for (int isH = 0; isH < 2; ++isH) {
-        std::map<int64_t, std::vector<InjContrib>> per;  // key = idx * 8 + comp
-        std::vector<int64_t> keys;                      // first-seen order
+        std::vector<Item> items;  // in the reference's face order
         for (int oi = 0; oi < 6; ++oi) {
             const int f = order[oi], ax = f / 2, far = f & 1;
             int u1, u2, v1, v2;
@@ -868,25 +891,25 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
                         c.coef = coef;
                         c.face = f;
                         c.pad = 0;
-                        const int64_t key = d.idx(i, j, k) * 8 + comp;
-                        auto it = per.find(key);
-                        if (it == per.end()) { keys.push_back(key); per[key].push_back(c); }
-                        else it->second.push_back(c);
+                        items.push_back({d.idx(i, j, k) * 8 + comp, c});
                     }
             }
         }
+        // targets in device order, so neighbouring threads touch neighbouring cells;
+        // the stable sort keeps each target's contributions in the reference's face order
+        std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.key < b.key; });
         std::vector<InjTarget> tg;
         std::vector<InjContrib> ct;
-        // targets in device order, so neighbouring threads touch neighbouring cells;
-        // each target keeps its contributions in the reference's face order
-        std::sort(keys.begin(), keys.end());
-        for (int64_t key : keys) {
-            const std::vector<InjContrib> &v = per[key];
+        ct.reserve(items.size());
+        for (size_t q = 0; q < items.size();) {
+            size_t r = q;
+            while (r < items.size() && items[r].key == items[q].key) ct.push_back(items[r++].c);
             InjTarget t;
-            t.idx = key / 8; t.comp = (int)(key % 8); t.start = (int32_t)ct.size(); t.count = (int32_t)v.size();
-            t.face = v[0].face;
+            t.idx = items[q].key / 8; t.comp = (int)(items[q].key % 8);
+            t.start = (int32_t)(ct.size() - (r - q)); t.count = (int32_t)(r - q);
+            t.face = items[q].c.face;
             tg.push_back(t);
-            ct.insert(ct.end(), v.begin(), v.end());
+            q = r;
         }
         const int side = isH;  // d_tg[0] = E targets, d_tg[1] = H targets
         g->ntg[side] = (int)tg.size();
@@ -1247,9 +1270,7 @@ extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
     }
     if (g->dl_on) CK(cudaMemsetAsync(g->d_dl_state, 0, (size_t)g->dl_n * 3 * g->dlc.stride * g->esz, g->stream));
     if (g->gain_on) {
-        std::vector<double> init;
-        gain_initial_state(g, init, g->g_n);
-        cps_status s = upload_real(g, g->d_g_state, init.data(), init.size());
+        cps_status s = gain_state_init(g);
         if (s) return s;
     }
     for (PortState &P : g->ports) {

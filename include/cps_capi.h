@@ -308,6 +308,44 @@ CPS_API cps_status cps_batch_tune_key(const cps_batch *b, char *buf, int32_t len
 CPS_API cps_status cps_batch_autotune(cps_batch *b, const char *cache_path, int32_t trial_steps,
                                       int32_t *steps_run);
 
+/* ---- serving loop (no reference counterpart).  Jobs are queued with an
+ * admission footprint and a step count; a poll builds the queued jobs that
+ * fit (free slot and used + footprint <= budget, first come first served),
+ * waits for the chunk in flight, retires finished jobs and launches the next
+ * chunk for every live job in one batch (continuous batching).  build creates
+ * and sets up the job's grid when it is admitted (a failing build fails that
+ * job only); done receives the grid when the job ends -- status CPS_OK,
+ * CPS_E_BUDGET (larger than the whole budget), CPS_E_CANCELLED, or the error
+ * that ended it -- and must copy out what it needs: the server destroys the
+ * grid when done returns.  A job's results do not depend on the other jobs. */
+typedef struct cps_server cps_server;
+typedef cps_status (*cps_job_build_fn)(void *user, int64_t job_id, cps_grid **out);
+typedef void (*cps_job_done_fn)(void *user, int64_t job_id, cps_grid *g, cps_status status);
+typedef struct cps_server_config {
+    int32_t precision;       /* CPS_FP32 or CPS_FP64: every job's grid */
+    int32_t max_jobs;        /* live jobs at most */
+    int64_t budget_bytes;    /* device memory admission budget */
+    int32_t chunk_steps;     /* steps between scheduling points, 1..64 */
+    int32_t tile_rows, tile_planes, tile_persistent;  /* batch tiling; rows 0 keeps the default */
+} cps_server_config;
+typedef struct cps_server_stats {
+    int64_t jobs_done, jobs_failed, jobs_rejected, jobs_cancelled, jobs_live, jobs_queued;
+    int64_t bytes_in_use, chunks;
+    double latency_p50_ms, latency_p99_ms;   /* submit -> done, finished jobs */
+    double wait_p50_ms, wait_p99_ms;         /* submit -> admitted */
+    double run_p50_ms;                       /* admitted -> done */
+    double cell_updates;                     /* of all chunks completed */
+    double span_s;                           /* first submit -> last finished job */
+} cps_server_stats;
+CPS_API cps_status cps_server_create(const cps_server_config *cfg, cps_server **out);
+CPS_API cps_status cps_server_destroy(cps_server *s);   /* cancels what is left */
+CPS_API cps_status cps_server_submit(cps_server *s, int64_t footprint_bytes, int32_t nsteps,
+                                     cps_job_build_fn build, cps_job_done_fn done, void *user, int64_t *job_id);
+CPS_API cps_status cps_server_poll(cps_server *s, int32_t *live, int32_t *queued);
+CPS_API cps_status cps_server_drain(cps_server *s);      /* poll until nothing is queued or live */
+CPS_API cps_status cps_server_cancel(cps_server *s, int64_t job_id);
+CPS_API cps_status cps_server_get_stats(const cps_server *s, cps_server_stats *out);
+
 #ifdef __cplusplus
 }
 #endif
