@@ -207,7 +207,9 @@ def run_ref_harness(dk, workdir=None, record_ports=False, exe=None, timeout=600)
     out_dir = os.path.join(workdir, "out")
     os.makedirs(out_dir, exist_ok=True)
     dk.write(deck_dir, record_ports=record_ports)
-    r = subprocess.run([exe or REF_HARNESS, deck_dir, out_dir], capture_output=True, text=True, timeout=timeout)
+    # cwd: the reference's CW-mode TF/SF writes Pout.txt into the working directory
+    r = subprocess.run([exe or REF_HARNESS, deck_dir, out_dir], capture_output=True, text=True, timeout=timeout,
+                       cwd=out_dir)
     if r.returncode != 0:
         raise RuntimeError(f"ref_harness failed ({r.returncode}): {r.stderr[-2000:]}")
     info = {}
@@ -249,7 +251,8 @@ def ref_bench(dk, warm, timed, threads=0, exe=None, timeout=900):
     try:
         deck_dir = os.path.join(workdir, "deck")
         dk.write(deck_dir, bench=(warm, timed), threads=threads)
-        r = subprocess.run([exe or REF_BENCH, deck_dir, workdir], capture_output=True, text=True, timeout=timeout)
+        r = subprocess.run([exe or REF_BENCH, deck_dir, workdir], capture_output=True, text=True, timeout=timeout,
+                           cwd=workdir)
         if r.returncode != 0:
             raise RuntimeError(f"ref_bench failed ({r.returncode}): {r.stderr[-2000:]}")
         for line in r.stdout.splitlines():
