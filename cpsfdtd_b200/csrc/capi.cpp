@@ -519,6 +519,30 @@ extern "C" cps_status cps_grid_info(const cps_grid *g, cps_grid_desc *out)
     return CPS_OK;
 }
 
+extern "C" cps_status cps_grid_coefficients(const cps_grid *g, double *aE, double *bE, double *aH, double *bH)
+{
+    REQUIRE(g, CPS_E_INVALID, "cps_grid_coefficients: NULL grid");
+    REQUIRE(g->nmedia > 0, CPS_E_STATE, "cps_grid_coefficients: media are not set");
+    for (int m = 0; m < g->nmedia; ++m) {
+        if (aE) aE[m] = g->aE[m];
+        if (bE) bE[m] = g->bE[m];
+        if (aH) aH[m] = g->aH[m];
+        if (bH) bH[m] = g->bH[m];
+    }
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_stretch(const cps_grid *g, int32_t which, double *out, int32_t *len)
+{
+    REQUIRE(g, CPS_E_INVALID, "cps_grid_stretch: NULL grid");
+    REQUIRE(which >= 0 && which < 12, CPS_E_INVALID, "cps_grid_stretch: which is 0..11");
+    const int n = kStretchLen(g, which);
+    if (len) *len = n;
+    if (out)
+        for (int q = 0; q < n; ++q) out[q] = q < (int)g->st[which].size() ? g->st[which][q] : 0.0;
+    return CPS_OK;
+}
+
 extern "C" cps_status cps_grid_bytes(const cps_grid *g, int64_t *bytes)
 {
     REQUIRE(g && bytes, CPS_E_INVALID, "NULL argument");

@@ -270,6 +270,13 @@ CPS_API cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *
  * registers.  Both give the same results. */
 CPS_API cps_status cps_grid_set_sweep(cps_grid *g, int32_t mode);
 CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sweep_ms, int64_t *samples);
+/* host FP64 copies of the per-medium coefficients (Structure::aE, bE, aH,
+ * bH, Structure.cpp:309-359), NoMedia entries each; NULL skips an array */
+CPS_API cps_status cps_grid_coefficients(const cps_grid *g, double *aE, double *bE, double *aH, double *bH);
+/* one stretched-coordinate array (Structure.h:82-83) with the CPML kappa
+ * folded in: which = 0..11 for cExy cEyx cEzx cExz cEzy cEyz cHxy cHyx cHzx
+ * cHxz cHzy cHyz; *len receives its length (Nz, Ny or Nx); out may be NULL */
+CPS_API cps_status cps_grid_stretch(const cps_grid *g, int32_t which, double *out, int32_t *len);
 
 /* ---- batched engine (no reference counterpart: main.cpp runs one grid per
  * process).  A batch advances many independent grids of one precision

@@ -1,0 +1,80 @@
+"""The C++ drop-in classes (include/cpsfdtd_classes.hpp): a main.cpp in the
+reference's style builds against them and the library, reads the reference's
+deck formats, and on the GPU gives the oracle's results for the same decks in
+the same call order."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from cpsfdtd_b200 import decks
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIBDIR = os.path.join(ROOT, "cpsfdtd_b200")
+
+
+def _build(tmp_path):
+    import cpsfdtd_b200 as cps
+    cps.lib()  # the library must exist
+    exe = str(tmp_path / "dropin")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+           os.path.join(ROOT, "tests", "dropin", "main.cpp"), "-L", LIBDIR, "-lcpsfdtd",
+           "-Wl,-rpath," + LIBDIR, "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_dropin_main_builds_and_fails_loudly(tmp_path):
+    exe = _build(tmp_path)
+    r = subprocess.run([exe, str(tmp_path / "no_such_deck"), "3", str(tmp_path)], capture_output=True, text=True)
+    assert r.returncode == 1 and "cannot open deck" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["dispersive", "dielectric"])
+def test_dropin_matches_oracle(tmp_path, oracle_mod, case):
+    import cpsfdtd_b200 as cps
+    exe = _build(tmp_path)
+    if case == "dispersive":
+        dk = decks.config2(n=32, steps=40, nfreq=2)
+    else:
+        dk = decks.config1(n=28, steps=40)
+        dk.sources = []  # point sources are main.cpp code, not a class: drive it with a TF/SF beam instead
+        dk.tfsf = decks.config2(n=28, steps=40, nfreq=1).tfsf
+    deck = tmp_path / "deck"
+    out = tmp_path / "out"
+    os.makedirs(out)
+    dk.write(str(deck))
+    nsteps = 40
+    r = subprocess.run([exe, str(deck), str(nsteps), str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.startswith("dropin ok")
+
+    ids = cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    pts = [cps.port_points(dk, p) for p in dk.ports]
+    o = oracle_mod.Oracle.from_deck(dk, ids, pts)
+    L = o.L
+    for n in range(1, nsteps + 1):  # the call order of tests/dropin/main.cpp
+        L.orc_op_h_bulk(o.h)
+        L.orc_op_tfsf_h(o.h, n)
+        L.orc_op_h_pml(o.h)
+        L.orc_op_e_bulk(o.h)
+        if dk.dl:
+            L.orc_op_dl(o.h)
+        L.orc_op_tfsf_e(o.h, n)
+        L.orc_op_e_pml(o.h)
+        L.orc_op_ports(o.h, n)
+    shape = (dk.nx + 1, dk.ny + 1, dk.nz + 1)
+    for c in range(6):
+        got = np.fromfile(str(out / f"field{c}.bin"), dtype=np.float64).reshape(shape)
+        assert rel_l2(got, o.field(c)) < 1e-10, c
+    for q, p in enumerate(pts):
+        got = np.loadtxt(str(out / f"portE{q}.txt")).reshape(-1, 3)
+        ref = o.port_last(q)[:, :3]
+        assert got.shape == ref.shape
+        assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max() + 1e-300
+        ijk = np.loadtxt(str(out / f"portP{q}.txt"), dtype=np.int64).reshape(-1, 3)
+        assert np.array_equal(ijk, p)
