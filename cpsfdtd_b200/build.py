@@ -35,6 +35,7 @@ SOURCES = {
     "kernels_batch.cu": [],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
+    "noalloc.cu": [],
 }
 
 

@@ -270,6 +270,13 @@ CPS_API cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *
  * registers.  Both give the same results. */
 CPS_API cps_status cps_grid_set_sweep(cps_grid *g, int32_t mode);
 CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sweep_ms, int64_t *samples);
+/* cps_ports_flush without any device allocation (no reference counterpart):
+ * the contraction's phasor scratch is a 512 KiB static device array shared by
+ * all grids of a device, so ports may have at most 256 frequencies and calls
+ * on one device must not overlap.  For callers that cannot allocate (a fixed
+ * admitted memory budget, or a loop that must not enter the allocator).  The
+ * first call on a device looks up the array's address. */
+CPS_API cps_status cps_ports_flush_static(cps_grid *g);
 /* host FP64 copies of the per-medium coefficients (Structure::aE, bE, aH,
  * bH, Structure.cpp:309-359), NoMedia entries each; NULL skips an array */
 CPS_API cps_status cps_grid_coefficients(const cps_grid *g, double *aE, double *bE, double *aH, double *bH);
