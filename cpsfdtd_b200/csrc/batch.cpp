@@ -67,7 +67,9 @@ bool tile_in_pml_host(const int np[6], const Dims &d, int x0, int y0, int by, in
     return x || y || z;
 }
 
-enum { kHInt, kHPml, kEInt, kEPml, kEIntGain, kEPmlGain, kNumSweep };
+// sweep classes: H interior / H CPML tiles, then E tiles by class bits
+// (1 CPML tile, 2 Drude-Lorentz grid, 4 gain grid)
+enum { kHInt, kHPml, kE0, kNumSweep = kE0 + 8 };
 
 }  // namespace
 
@@ -218,7 +220,7 @@ cps_status rebuild_T(cps_batch *b)
         const Dims &d = g->d;
         b->cells += (int64_t)d.nx * d.ny * d.nz;
         // sweep tiles, z outermost so that neighbouring blocks share halos
-        const bool gain = B.G.on && B.G.ncell > 0;
+        const bool gain = B.G.on && B.G.ncell > 0, dlg = B.D.on && B.D.ncell > 0;
         const int nbx = cdiv_i(d.nx, 32), nby = cdiv_i(d.ny, by), nbz = cdiv_i(d.nz, kc);
         for (int bz = 0; bz < nbz; ++bz)
             for (int yb = 0; yb < nby; ++yb)
@@ -235,8 +237,7 @@ cps_status rebuild_T(cps_batch *b)
                         const int k0 = std::max(1, bz * kc), k1 = std::min(bz * kc + kc, d.nz);
                         if (k0 < k1) {
                             const bool pml = B.p.on && tile_in_pml_host(B.p.np, d, xb * 32, yb * by, by, k0, k1, true);
-                            const int cls = gain ? (pml ? kEPmlGain : kEIntGain) : (pml ? kEPml : kEInt);
-                            tiles[cls].push_back(t);
+                            tiles[kE0 + (pml ? 1 : 0) + (dlg ? 2 : 0) + (gain ? 4 : 0)].push_back(t);
                         }
                     }
                 }
@@ -295,9 +296,9 @@ cps_status rebuild_T(cps_batch *b)
         b->ntiles[c] = (int)tiles[c].size();
         b->nblocks[c] = b->ntiles[c];
         if (b->persistent && b->ntiles[c] > 0) {
-            const bool eside = c >= kEInt, pml = c == kHPml || c == kEPml || c == kEPmlGain;
-            const bool gain = c == kEIntGain || c == kEPmlGain;
-            const int per_sm = batch_blocks_per_sm<T>(by, eside, pml, gain);
+            const bool eside = c >= kE0;
+            const int cls = eside ? c - kE0 : (c == kHPml ? 1 : 0);
+            const int per_sm = batch_blocks_per_sm<T>(by, eside, cls);
             b->nblocks[c] = std::min(b->ntiles[c], per_sm * nsm);
         }
     }
@@ -335,12 +336,8 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_h_batch<T>(G, b->d_tiles[kHInt], b->ntiles[kHInt], b->nblocks[kHInt], b->by, false, b->d_err, st);
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
         launch_inject_batch<T>(G, b->d_inj[1], b->ninj[1], 1, s, st);
-        launch_e_batch<T>(G, b->d_tiles[kEInt], b->ntiles[kEInt], b->nblocks[kEInt], b->by, false, false, b->d_err, st);
-        launch_e_batch<T>(G, b->d_tiles[kEPml], b->ntiles[kEPml], b->nblocks[kEPml], b->by, true, false, b->d_err, st);
-        launch_e_batch<T>(G, b->d_tiles[kEIntGain], b->ntiles[kEIntGain], b->nblocks[kEIntGain], b->by, false, true,
-                          b->d_err, st);
-        launch_e_batch<T>(G, b->d_tiles[kEPmlGain], b->ntiles[kEPmlGain], b->nblocks[kEPmlGain], b->by, true, true,
-                          b->d_err, st);
+        for (int c = 0; c < 8; ++c)
+            launch_e_batch<T>(G, b->d_tiles[kE0 + c], b->ntiles[kE0 + c], b->nblocks[kE0 + c], b->by, c, b->d_err, st);
         launch_dl_batch<T>(G, b->d_dl, b->ndl, st);
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);

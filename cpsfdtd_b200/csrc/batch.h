@@ -64,9 +64,10 @@ constexpr int kMaxRing = 64;  // samples per port ring = longest chunk
 template <typename T>
 void launch_h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, bool pml,
                     int *err, cudaStream_t s);
+// cls bits: 1 CPML tiles, 2 Drude-Lorentz grids, 4 gain grids
 template <typename T>
-void launch_e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, bool pml,
-                    bool gain, int *err, cudaStream_t s);
+void launch_e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, int cls, int *err,
+                    cudaStream_t s);
 template <typename T>
 void launch_dl_batch(const BatchGrid<T> *grids, const int4 *blocks, int nblocks, cudaStream_t s);
 template <typename T>
@@ -89,6 +90,6 @@ template <typename T>
 void dft_batch_attributes();
 // sweep blocks of one SM that fit at once (for persistent launches)
 template <typename T>
-int batch_blocks_per_sm(int by, bool eside, bool pml, bool gain);
+int batch_blocks_per_sm(int by, bool eside, int cls);
 
 }  // namespace cps

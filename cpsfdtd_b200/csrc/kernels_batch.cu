@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(32 * BY) k_h_batch(const BatchGrid<T> *__restr
     }
 }
 
-template <typename T, int BY, bool PML, bool GAIN>
+template <typename T, int BY, bool PML, bool GAIN, bool DL>
 __global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restrict__ grids,
                                                       const int4 *__restrict__ tiles, int ntiles, int *err)
 {
@@ -74,13 +74,9 @@ __global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restr
             if (lead) acquire_maps(B.M);
             last = e.x;
         }
-        const TileXYZ t{e.y, e.z, e.w};
-        bool ok;
-        if (B.D.on && B.D.ncell > 0)
-            ok = e_tma_body<T, BY, PML, true, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, t, ctr, err, sm, full);
-        else
-            ok = e_tma_body<T, BY, PML, false, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, t, ctr, err, sm, full);
-        if (!ok) return;
+        if (!e_tma_body<T, BY, PML, DL, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm,
+                                               full))
+            return;
     }
 }
 
@@ -123,14 +119,6 @@ void h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nbloc
     k_h_batch<T, BY, PML><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
 }
 
-template <typename T, int BY, bool PML, bool GAIN>
-void e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
-{
-    using L = StageLayout<T, BY>;
-    smem_attr<k_e_batch<T, BY, PML, GAIN>>(L::SMEM);
-    k_e_batch<T, BY, PML, GAIN><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
-}
-
 template <typename K>
 int occupancy(K kernel, int threads, int smem)
 {
@@ -141,6 +129,60 @@ int occupancy(K kernel, int threads, int smem)
         return 1;
     }
     return n > 0 ? n : 1;
+}
+
+template <typename T, int BY, bool PML, bool GAIN, bool DL>
+void e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
+{
+    using L = StageLayout<T, BY>;
+    smem_attr<k_e_batch<T, BY, PML, GAIN, DL>>(L::SMEM);
+    k_e_batch<T, BY, PML, GAIN, DL><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
+}
+
+template <typename T, int BY>
+void e_batch_by(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int cls, int *err,
+                cudaStream_t s)
+{
+    switch (cls & 7) {
+    case 0: e_batch<T, BY, false, false, false>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 1: e_batch<T, BY, true, false, false>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 2: e_batch<T, BY, false, false, true>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 3: e_batch<T, BY, true, false, true>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 4: e_batch<T, BY, false, true, false>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 5: e_batch<T, BY, true, true, false>(grids, tiles, ntiles, nblocks, err, s); break;
+    case 6: e_batch<T, BY, false, true, true>(grids, tiles, ntiles, nblocks, err, s); break;
+    default: e_batch<T, BY, true, true, true>(grids, tiles, ntiles, nblocks, err, s); break;
+    }
+}
+
+template <typename T, int BY>
+void e_batch_attrs()
+{
+    using L = StageLayout<T, BY>;
+    smem_attr<k_e_batch<T, BY, false, false, false>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, true, false, false>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, false, false, true>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, true, false, true>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, false, true, false>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, true, true, false>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, false, true, true>>(L::SMEM);
+    smem_attr<k_e_batch<T, BY, true, true, true>>(L::SMEM);
+}
+
+template <typename T, int BY>
+int e_batch_occupancy(int cls)
+{
+    using L = StageLayout<T, BY>;
+    switch (cls & 7) {
+    case 0: return occupancy(k_e_batch<T, BY, false, false, false>, 32 * BY, L::SMEM);
+    case 1: return occupancy(k_e_batch<T, BY, true, false, false>, 32 * BY, L::SMEM);
+    case 2: return occupancy(k_e_batch<T, BY, false, false, true>, 32 * BY, L::SMEM);
+    case 3: return occupancy(k_e_batch<T, BY, true, false, true>, 32 * BY, L::SMEM);
+    case 4: return occupancy(k_e_batch<T, BY, false, true, false>, 32 * BY, L::SMEM);
+    case 5: return occupancy(k_e_batch<T, BY, true, true, false>, 32 * BY, L::SMEM);
+    case 6: return occupancy(k_e_batch<T, BY, false, true, true>, 32 * BY, L::SMEM);
+    default: return occupancy(k_e_batch<T, BY, true, true, true>, 32 * BY, L::SMEM);
+    }
 }
 
 }  // namespace
@@ -161,28 +203,13 @@ void launch_h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, in
 }
 
 template <typename T>
-void launch_e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, bool pml,
-                    bool gain, int *err, cudaStream_t s)
+void launch_e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int by, int cls, int *err,
+                    cudaStream_t s)
 {
     if (ntiles <= 0) return;
     if (nblocks <= 0 || nblocks > ntiles) nblocks = ntiles;
-    if (by == 4) {
-        if (pml) {
-            if (gain) e_batch<T, 4, true, true>(grids, tiles, ntiles, nblocks, err, s);
-            else e_batch<T, 4, true, false>(grids, tiles, ntiles, nblocks, err, s);
-        } else {
-            if (gain) e_batch<T, 4, false, true>(grids, tiles, ntiles, nblocks, err, s);
-            else e_batch<T, 4, false, false>(grids, tiles, ntiles, nblocks, err, s);
-        }
-    } else {
-        if (pml) {
-            if (gain) e_batch<T, 8, true, true>(grids, tiles, ntiles, nblocks, err, s);
-            else e_batch<T, 8, true, false>(grids, tiles, ntiles, nblocks, err, s);
-        } else {
-            if (gain) e_batch<T, 8, false, true>(grids, tiles, ntiles, nblocks, err, s);
-            else e_batch<T, 8, false, false>(grids, tiles, ntiles, nblocks, err, s);
-        }
-    }
+    if (by == 4) e_batch_by<T, 4>(grids, tiles, ntiles, nblocks, cls, err, s);
+    else e_batch_by<T, 8>(grids, tiles, ntiles, nblocks, cls, err, s);
 }
 
 template <typename T>
@@ -200,24 +227,18 @@ void launch_advance_batch(BatchGrid<T> *grids, int ngrids, int nsteps, cudaStrea
 }
 
 template <typename T>
-int batch_blocks_per_sm(int by, bool eside, bool pml, bool gain)
+int batch_blocks_per_sm(int by, bool eside, int cls)
 {
     if (by == 4) {
         using L = StageLayout<T, 4>;
-        if (!eside) return pml ? occupancy(k_h_batch<T, 4, true>, 128, L::SMEM)
-                               : occupancy(k_h_batch<T, 4, false>, 128, L::SMEM);
-        if (pml) return gain ? occupancy(k_e_batch<T, 4, true, true>, 128, L::SMEM)
-                             : occupancy(k_e_batch<T, 4, true, false>, 128, L::SMEM);
-        return gain ? occupancy(k_e_batch<T, 4, false, true>, 128, L::SMEM)
-                    : occupancy(k_e_batch<T, 4, false, false>, 128, L::SMEM);
+        if (!eside) return (cls & 1) ? occupancy(k_h_batch<T, 4, true>, 128, L::SMEM)
+                                     : occupancy(k_h_batch<T, 4, false>, 128, L::SMEM);
+        return e_batch_occupancy<T, 4>(cls);
     }
     using L = StageLayout<T, 8>;
-    if (!eside) return pml ? occupancy(k_h_batch<T, 8, true>, 256, L::SMEM)
-                           : occupancy(k_h_batch<T, 8, false>, 256, L::SMEM);
-    if (pml) return gain ? occupancy(k_e_batch<T, 8, true, true>, 256, L::SMEM)
-                         : occupancy(k_e_batch<T, 8, true, false>, 256, L::SMEM);
-    return gain ? occupancy(k_e_batch<T, 8, false, true>, 256, L::SMEM)
-                : occupancy(k_e_batch<T, 8, false, false>, 256, L::SMEM);
+    if (!eside) return (cls & 1) ? occupancy(k_h_batch<T, 8, true>, 256, L::SMEM)
+                                 : occupancy(k_h_batch<T, 8, false>, 256, L::SMEM);
+    return e_batch_occupancy<T, 8>(cls);
 }
 
 template <typename T>
@@ -227,25 +248,19 @@ void batch_kernel_attributes()
     smem_attr<k_h_batch<T, 4, true>>(StageLayout<T, 4>::SMEM);
     smem_attr<k_h_batch<T, 8, false>>(StageLayout<T, 8>::SMEM);
     smem_attr<k_h_batch<T, 8, true>>(StageLayout<T, 8>::SMEM);
-    smem_attr<k_e_batch<T, 4, false, false>>(StageLayout<T, 4>::SMEM);
-    smem_attr<k_e_batch<T, 4, false, true>>(StageLayout<T, 4>::SMEM);
-    smem_attr<k_e_batch<T, 4, true, false>>(StageLayout<T, 4>::SMEM);
-    smem_attr<k_e_batch<T, 4, true, true>>(StageLayout<T, 4>::SMEM);
-    smem_attr<k_e_batch<T, 8, false, false>>(StageLayout<T, 8>::SMEM);
-    smem_attr<k_e_batch<T, 8, false, true>>(StageLayout<T, 8>::SMEM);
-    smem_attr<k_e_batch<T, 8, true, false>>(StageLayout<T, 8>::SMEM);
-    smem_attr<k_e_batch<T, 8, true, true>>(StageLayout<T, 8>::SMEM);
+    e_batch_attrs<T, 4>();
+    e_batch_attrs<T, 8>();
     dft_batch_attributes<T>();
 }
 
 #define CPS_BATCH_INSTANTIATE(T)                                                                             \
     template void launch_h_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, bool, int *,          \
                                     cudaStream_t);                                                           \
-    template void launch_e_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, bool, bool, int *,   \
+    template void launch_e_batch<T>(const BatchGrid<T> *, const int4 *, int, int, int, int, int *,          \
                                     cudaStream_t);                                                           \
     template void launch_dl_batch<T>(const BatchGrid<T> *, const int4 *, int, cudaStream_t);                 \
     template void launch_advance_batch<T>(BatchGrid<T> *, int, int, cudaStream_t);                           \
-    template int batch_blocks_per_sm<T>(int, bool, bool, bool);                                              \
+    template int batch_blocks_per_sm<T>(int, bool, int);                                              \
     template void batch_kernel_attributes<T>();
 CPS_BATCH_INSTANTIATE(float)
 CPS_BATCH_INSTANTIATE(double)

@@ -128,7 +128,7 @@ __device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_dft(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
+__global__ void __launch_bounds__(256, 2) k_dft(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
                                              const int32_t *comps, double *acc)
 {
     extern __shared__ __align__(16) unsigned char sh_raw[];
@@ -171,7 +171,7 @@ __global__ void k_phasors_batch(const BatchGrid<T> *__restrict__ grids, const Ba
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_dft_batch(const BatchPort<T> *__restrict__ ports,
+__global__ void __launch_bounds__(256, 2) k_dft_batch(const BatchPort<T> *__restrict__ ports,
                                                    const int4 *__restrict__ blocks, int nslots)
 {
     extern __shared__ __align__(16) unsigned char sh_raw[];
