@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="grid edge (cells)")
+    ap.add_argument("--workload", default="dispersive", choices=["dispersive", "laser"],
+                    help="bench deck: dispersive scattering (default) or the photonic-crystal laser")
     ap.add_argument("--job-steps", type=int, default=4000)
     ap.add_argument("--e2e-steps", type=int, default=2, help="end-to-end jobs to time")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
@@ -118,16 +120,52 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(n, job_steps):
+def workload(n, job_steps, kind="dispersive"):
+    """The bench deck: the dispersive-scattering deck (default), or the
+    disordered photonic-crystal laser deck (four-level gain, 32-frequency
+    spherical-port DFT)."""
     from cpsfdtd_b200 import decks
+    if kind == "laser":
+        return decks.config3(n=n, steps=job_steps, seed=0, nfreq=32)
     return decks.config2(n=n, steps=job_steps, nfreq=64)
 
 
-def sweep_bytes(dk, ndl, prec_bytes=4):
+def workload_name(dk, kind):
+    if kind == "laser":
+        return (f"disordered photonic-crystal laser {dk.nx}^3, eps 11.9 spheres in gain-doped eps 2.25, CPML "
+                f"{dk.pml['npml'][0]}, Ez seed pulse, spherical port x 32-freq FP64 DFT; 1 bench step = 1 job of "
+                f"{dk.nsteps} time steps")
+    return (f"dispersive scattering {dk.nx}^3, Drude-Lorentz 4x4x4 spheres, CPML {dk.pml['npml'][0]}, TF/SF "
+            f"Gaussian beam, 6 ports x 64-freq FP64 DFT; 1 bench step = 1 job of {dk.nsteps} time steps")
+
+
+def config_of(dk, kind, world):
+    return {"workload": workload_name(dk, kind), "grid": [dk.nx, dk.ny, dk.nz], "time_steps_per_job": dk.nsteps,
+            "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
+            "l2": f"inputs larger than L2 (fields {6 * 4 * (dk.nx + 1) * (dk.ny + 1) * (dk.nz + 1) / 1e9:.2f} GB "
+                  "per grid)", "parallelism": f"replicas x{world}"}
+
+
+def aggregate(units_local, ms_local, dist=None, device=None):
+    """Whole-job throughput of replicas: units summed over ranks / the slowest
+    rank's time (max over ranks); returns (units per second, max ms)."""
+    if dist is None:
+        return units_local / (ms_local / 1e3), ms_local
+    import torch
+    t = torch.tensor([ms_local, units_local], dtype=torch.float64, device=device)
+    mx = t[:1].clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    tot = t[1:].clone()
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return float(tot.item()) / (float(mx.item()) / 1e3), float(mx.item())
+
+
+def sweep_bytes(dk, ndl, prec_bytes=4, ngain=0):
     """Algorithmic bytes of one H sweep and one E sweep (FP32): each field word
     read and written once, 1 B material ID, CPML psi (2 words read+write per
     slab cell per sweep), Drude-Lorentz state (3 x (nD + 2 nL + 1) words read
-    + write per ID-2 cell).  Neighbour re-reads are not counted."""
+    + write per ID-2 cell), gain state (12 polarisation + 3 population words
+    read + write per gain cell).  Neighbour re-reads are not counted."""
     nx, ny, nz, s = dk.nx, dk.ny, dk.nz, prec_bytes
     np_ = dk.pml["npml"][0] if dk.pml else 0
     h_cells = nx * ny * nz
@@ -137,7 +175,7 @@ def sweep_bytes(dk, ndl, prec_bytes=4):
     psi = 2 * 2 * s
     h = h_cells * (9 * s + 1) + h_slab * psi
     stride = len(dk.dl["fD"]) + 2 * len(dk.dl["fL"]) + 1 if dk.dl else 0
-    e = e_cells * (9 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s
+    e = e_cells * (9 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s + ngain * 15 * 2 * s
     return h, e
 
 
@@ -155,7 +193,7 @@ def dist_setup():
     return world, rank, local, dist
 
 
-def cpu_baseline(dk, steps):
+def cpu_baseline(dk, steps, deck_kind="dispersive"):
     """The reference's own code on the same deck, bounded sample on all host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -163,8 +201,9 @@ def cpu_baseline(dk, steps):
     if os.path.exists(oracle.REF_BENCH):
         r = oracle.ref_bench(dk, 1, steps, threads=threads)
         kind = "reference"
+        extra = "3-D Drude-Lorentz" if deck_kind == "dispersive" else "3-D four-level gain"
         sample = (f"{dk.nx}^3 deck, {steps} time steps after 1 warm-up, reference BasicFDTD/CPML/TF_SF/Ports "
-                  f"(OpenMP) + 3-D Drude-Lorentz from the oracle restatement")
+                  f"(OpenMP) + {extra} from the oracle restatement")
     else:
         o = oracle.Oracle.from_deck(dk, _ids(dk))
         oracle.Oracle.threads(threads)
@@ -193,13 +232,14 @@ def run_reference(args):
     world, rank, local, dist = dist_setup()
     if rank != 0:
         return
-    dk = workload(args.n, args.job_steps)
+    dk = workload(args.n, args.job_steps, args.workload)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
     if os.path.exists(oracle.REF_BENCH):
         r = oracle.ref_bench(dk, args.warmup, args.steps, threads=threads)
-        kind, what = "reference", "reference BasicFDTD/CPML/TF_SF/Ports (OpenMP) + 3-D Drude-Lorentz from the oracle restatement"
+        extra = "3-D Drude-Lorentz" if args.workload == "dispersive" else "3-D four-level gain"
+        kind, what = "reference", f"reference BasicFDTD/CPML/TF_SF/Ports (OpenMP) + {extra} from the oracle restatement"
     else:
         o = oracle.Oracle.from_deck(dk, _ids(dk))
         oracle.Oracle.threads(threads)
@@ -209,12 +249,13 @@ def run_reference(args):
         r = {"cells": dk.cells, "steps": args.steps, "seconds": time.perf_counter() - t0, "threads": threads}
         kind, what = "port", "oracle restatement (OpenMP)"
     v = r["cells"] * r["steps"] / r["seconds"] / 1e9
-    sample = f"{dk.nx}^3 dispersive-scattering deck, {args.steps} time steps after {args.warmup} warm-up, {what}"
+    sample = (f"{dk.nx}^3 {args.workload} deck: each bench step is 1 time step of the job (bounded sample), "
+              f"{args.steps} timed after {args.warmup} warm-up, {what}")
     line = {"metric": "Gcell-upd/s", "value": v, "unit": "Gcell-upd/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded deck generator)",
-            "config": {"workload": f"dispersive scattering {dk.nx}^3 (1 bench step = 1 time step on CPU)"},
+            "config": config_of(dk, args.workload, args.gpus),
             "cpu_baseline": {"value": v, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -258,12 +299,8 @@ def ensemble(args, local, dist):
     b.step(args.ens_steps)
     e1.record(stream)
     b.sync()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    batched = cells * args.ens_steps / (ms / 1e3) / 1e9
+    batched, ms = aggregate(cells * args.ens_steps, e0.elapsed_time(e1), dist, f"cuda:{local}")
+    batched /= 1e9
     launches = b.launches() - l0
     tile = list(b.get_tile())
     b.close()
@@ -409,7 +446,7 @@ def run_ours(args):
     world, rank, local, dist = dist_setup()
     import cpsfdtd_b200 as cps
     torch.cuda.set_device(local)
-    dk = workload(args.n, args.job_steps)
+    dk = workload(args.n, args.job_steps, args.workload)
     ids = _ids(dk)
     pts = [cps.port_points(dk, p) for p in dk.ports]
     g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts, device=local)
@@ -445,20 +482,17 @@ def run_ours(args):
     launches = g.launches() - launches0
     h_ms, e_ms, nsamp = g.timing()
     g.set_timing(0)
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     cells = dk.cells
-    total = cells * dk.nsteps * args.steps * world
-    value = total / (ms / 1e3) / 1e9
+    value, ms = aggregate(cells * dk.nsteps * args.steps, ms, dist, f"cuda:{local}")
+    value /= 1e9
 
     # roofline of the dominant kernel (E sweep)
     P, src = peaks()
     ndl = 0
     from cpsfdtd_b200 import decks
-    ndl = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_DISPERSIVE).sum())
-    hb, eb = sweep_bytes(dk, ndl)
+    ndl = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_DISPERSIVE).sum()) if dk.dl else 0
+    ngain = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_GAIN).sum()) if dk.gain else 0
+    hb, eb = sweep_bytes(dk, ndl, ngain=ngain)
     dom_ms, dom_bytes, dom = (e_ms, eb, "E sweep") if e_ms >= h_ms else (h_ms, hb, "H sweep")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",
@@ -468,7 +502,7 @@ def run_ours(args):
             "step_bytes_per_cell": (hb + eb) / cells,
             "step_frac_at_50B": value / world * 50 / P["hbm_gbs"]}
     tr = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr):
+    if os.path.exists(tr) and args.workload == "dispersive" and args.n == 256:
         try:
             roof["traffic"] = json.load(open(tr)).get("e_sweep_bytes_per_launch")
         except (ValueError, OSError):
@@ -504,7 +538,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(workload(args.n, args.job_steps), args.cpu_steps)
+            cpu = cpu_baseline(workload(args.n, args.job_steps, args.workload), args.cpu_steps, args.workload)
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {ex}"}
@@ -525,12 +559,7 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
                 "data": "synthetic (seeded deck generator)",
-                "config": {"workload": f"dispersive scattering {dk.nx}^3, Drude-Lorentz 4x4x4 spheres, CPML "
-                                       f"{dk.pml['npml'][0]}, TF/SF Gaussian beam, 6 ports x 64-freq FP64 DFT; "
-                                       f"1 bench step = 1 job of {dk.nsteps} time steps",
-                           "grid": [dk.nx, dk.ny, dk.nz], "time_steps_per_job": dk.nsteps,
-                           "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
-                           "l2": "inputs larger than L2 (fields 0.40 GB per grid)", "parallelism": f"replicas x{world}"},
+                "config": config_of(dk, args.workload, world),
                 "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
                 "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens, "serving": srv}
         print(json.dumps(line), flush=True)
