@@ -145,22 +145,30 @@ void grade_h(std::vector<double> &kappa, std::vector<double> &b, std::vector<dou
 
 // sorted cell list (device linear index) of cells with a given ID inside the
 // E-update range, plus per (k, j, 32-wide x segment) start offsets
-cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cell, int32_t **d_seg)
+cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cell, int32_t **d_seg,
+                      uint2 **d_segm = nullptr)
 {
     const Dims &d = g->d;
     std::vector<int64_t> cells;
     const int nseg = d.px / 32;
     std::vector<int32_t> seg((size_t)(d.nz + 1) * (d.ny + 1) * nseg, 0);
+    std::vector<uint2> segm(d_segm ? seg.size() : 0);
     for (int k = 0; k <= d.nz; ++k)
         for (int j = 0; j <= d.ny; ++j)
             for (int s = 0; s < nseg; ++s) {
-                seg[((size_t)k * (d.ny + 1) + j) * nseg + s] = (int32_t)cells.size();
-                if (k < 1 || k >= d.nz || j < 1 || j >= d.ny) continue;
-                for (int i = s * 32; i < s * 32 + 32 && i < d.nx; ++i) {
-                    if (i < 1) continue;
-                    const int64_t q = d.idx(i, j, k);
-                    if (g->ids_dev[q] == id_match) cells.push_back(q);
-                }
+                const size_t w = ((size_t)k * (d.ny + 1) + j) * nseg + s;
+                seg[w] = (int32_t)cells.size();
+                uint32_t bits = 0;
+                if (k >= 1 && k < d.nz && j >= 1 && j < d.ny)
+                    for (int i = s * 32; i < s * 32 + 32 && i < d.nx; ++i) {
+                        if (i < 1) continue;
+                        const int64_t q = d.idx(i, j, k);
+                        if (g->ids_dev[q] == id_match) {
+                            cells.push_back(q);
+                            bits |= 1u << (i - s * 32);
+                        }
+                    }
+                if (d_segm) segm[w] = make_uint2((unsigned)seg[w], bits);
             }
     REQUIRE(cells.size() < (size_t)INT32_MAX, CPS_E_INVALID, "too many cells in one compacted list");
     *count = (int64_t)cells.size();
@@ -169,6 +177,10 @@ cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cel
     s = dalloc(g, (void **)d_seg, seg.size() * sizeof(int32_t));
     if (s) return s;
     if (!cells.empty()) { s = upload_raw(g, *d_cell, cells.data(), cells.size() * sizeof(int64_t)); if (s) return s; }
+    if (d_segm) {
+        if ((s = dalloc(g, (void **)d_segm, segm.size() * sizeof(uint2)))) return s;
+        if ((s = upload_raw(g, *d_segm, segm.data(), segm.size() * sizeof(uint2)))) return s;
+    }
     return upload_raw(g, *d_seg, seg.data(), seg.size() * sizeof(int32_t));
 }
 
@@ -790,7 +802,7 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     G.r_hwb = 1.0 / G.homega_bdt; G.r_hwa = 1.0 / G.homega_adt;
     G.inv_scale = 1.0 / G.scaleP;
     g->gain_id = p->gain_id;
-    if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg))) return s;
+    if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg, &g->d_g_segm))) return s;
     const int nw = g->fp32 ? kG32Words : kG64Words;
     if ((s = dalloc(g, &g->d_g_state, (size_t)g->g_n * nw * g->esz))) return s;
     if ((s = gain_state_init(g))) return s;

@@ -135,6 +135,7 @@ struct GainView {
     int64_t ncell;
     const int64_t *cell;
     const int32_t *seg;
+    const uint2 *segm;       // per (k, j, 32-wide x segment): list offset and the segment's gain-cell bit mask
     T *state;                // [word][ncell]
     GainCoef c;
 };

@@ -102,6 +102,7 @@ struct cps_grid {
     int64_t g_n = 0;
     int64_t *d_g_cell = nullptr;
     int32_t *d_g_seg = nullptr;
+    uint2 *d_g_segm = nullptr;
     void *d_g_state = nullptr;
     // TF/SF
     bool tfsf_on = false;
@@ -238,7 +239,7 @@ inline GainView<T> gain_view(const cps_grid *g)
     memset(&v, 0, sizeof(v));
     v.on = g->gain_on;
     if (!g->gain_on) return v;
-    v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg;
+    v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg; v.segm = g->d_g_segm;
     v.state = (T *)g->d_g_state; v.c = g->gc;
     return v;
 }

@@ -327,4 +327,70 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
     ex = E[0]; ey = E[1]; ez = E[2];
 }
 
+
+// ---- FP32 gain with the state fetched one plane ahead.  The list offset and
+// the bit mask of a warp row's gain cells come from the segment table, so a
+// plane's state can be loaded before its fields arrive; the arithmetic is
+// gain_warp's.
+struct GainRegs32 {
+    float pa[3], pa1[3], pb[3], pb1[3];
+    float n[3];  // N1 - 1, N2, N3
+};
+
+__device__ __forceinline__ uint2 gain_segment(const GainView<float> &G, const Dims &d, int j, int k, int seg,
+                                              bool rowok)
+{
+    return rowok ? __ldg(&G.segm[((int64_t)k * (d.ny + 1) + j) * (d.px >> 5) + seg]) : make_uint2(0u, 0u);
+}
+
+__device__ __forceinline__ void gain_fetch32(const GainView<float> &G, uint2 m, GainRegs32 &r)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    if (!((m.y >> lane) & 1u)) return;
+    using L = GainSite32;
+    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = G.ncell;
+    const float *st = G.state + c;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        r.pa[q] = __ldg(st + (L::PA + q) * sc);
+        r.pa1[q] = __ldg(st + (L::PA1 + q) * sc);
+        r.pb[q] = __ldg(st + (L::PB + q) * sc);
+        r.pb1[q] = __ldg(st + (L::PB1 + q) * sc);
+    }
+    r.n[0] = __ldg(st + L::DN1 * sc);
+    r.n[1] = __ldg(st + L::N2 * sc);
+    r.n[2] = __ldg(st + L::N3 * sc);
+}
+
+// P -> E -> N at this lane's cell when it is a gain cell of the segment
+__device__ __forceinline__ void gain_apply32(const GainView<float> &G, uint2 m, const GainRegs32 &r, float &ex,
+                                             float &ey, float &ez)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    if (!((m.y >> lane) & 1u)) return;
+    using L = GainSite32;
+    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = G.ncell;
+    float *st = G.state + c;
+    float E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
+    float Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) { Pa[q] = r.pa[q]; Pa1[q] = r.pa1[q]; Pb[q] = r.pb[q]; Pb1[q] = r.pb1[q]; }
+    double N[4];
+    N[1] = 1.0 + (double)r.n[0];
+    N[2] = (double)r.n[1];
+    N[3] = (double)r.n[2];
+    N[0] = 2.0 - N[1] - N[2] - N[3];  // FP64 conservation, FourLevelLaser.cpp:324
+    gain_p_update<float>(G.c, N, E, Pa, Pa1, Pa2, Pb, Pb1, Pb2);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) E[q] = gain_e_corr<float>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
+    gain_n_update<float>(G.c, N, E, E1, Pa, Pa1, Pa2, Pb, Pb2);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q];
+        st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q];
+    }
+    gain_store_n<float>(st, sc, N);
+    ex = E[0]; ey = E[1]; ez = E[2];
+}
+
 }  // namespace cps

@@ -128,9 +128,22 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         psi_load_e(p, d, pc, i, j, k0, qc);
         if (k0 + 1 < k1) psi_load_e(p, d, pc, i, j, k0 + 1, qn);
     }
+    // FP32 gain: state of plane k fetched during plane k-1, segment table two planes ahead
+    constexpr bool GPRE = GAIN && sizeof(T) == 4;
+    GainRegs32 gcur{}, gnext{};
+    uint2 mcur{0u, 0u}, mnext{0u, 0u}, mnn{0u, 0u};
+    if constexpr (GPRE) {
+        mcur = gain_segment(G, d, j, k0, t.bx, rowok);
+        if (k0 + 1 < k1) mnext = gain_segment(G, d, j, k0 + 1, t.bx, rowok);
+        gain_fetch32(G, mcur, gcur);
+    }
     const int hr = (ty + 1) * L::HW + tx + 4, orow = ty * L::OW + tx;
     for (int k = k0, it = 0; k < k1; ++k, ++it) {
         if (PML && act && k + 2 < k1) psi_load_e(p, d, pc, i, j, k + 2, qnn);
+        if constexpr (GPRE) {
+            mnn = k + 2 < k1 ? gain_segment(G, d, j, k + 2, t.bx, rowok) : make_uint2(0u, 0u);
+            if (k + 1 < k1) gain_fetch32(G, mnext, gnext);
+        }
         const uint32_t q = c0 + (uint32_t)it;
         const int s = (int)(q % kStages);
         const bool ok = wait_stage(&full[s], (q / kStages) & 1u);
@@ -158,7 +171,14 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
             ey = aE * ey + bE * dHx_k * cEyx - bE * dHz_i * cEyz;
             ez = aE * ez + bE * dHy_i * cEzy - bE * dHx_j * cEzx;
         }
-        if (GAIN && rowok) gain_warp(G, d, j, k, t.bx, act, id, ex, ey, ez);
+        if constexpr (GPRE) {
+            gain_apply32(G, mcur, gcur, ex, ey, ez);
+            gcur = gnext;
+            mcur = mnext;
+            mnext = mnn;
+        } else if (GAIN && rowok) {
+            gain_warp(G, d, j, k, t.bx, act, id, ex, ey, ez);
+        }
         // ID-2 cells are left untouched here: the Drude-Lorentz cell kernel
         // updates them (ADE, then CPML) after the sweep, in the reference order
         if (act && !(DL && id == CPS_ID_DISPERSIVE)) {
