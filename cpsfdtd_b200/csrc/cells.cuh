@@ -38,6 +38,32 @@ __device__ __forceinline__ T dl_component(const DlCoef<T> &D, T E, T curl, T *st
     return E;
 }
 
+// The same update for compile-time pole counts, from state words already in
+// registers (w[0 .. ND+2NL], the component's words in order); the arithmetic
+// is dl_component's, operation for operation.
+template <typename T, int ND, int NL>
+__device__ __forceinline__ T dl_component_regs(const DlCoef<T> &D, T E, T curl, const T *w, T *st, int64_t sc)
+{
+    const T temp = E;
+    T t1 = T(0), t2 = T(0);
+#pragma unroll
+    for (int p = 0; p < ND; ++p) t1 = t1 + D.C4[p] * w[p];
+#pragma unroll
+    for (int p = 0; p < NL; ++p) t2 = t2 + D.C5[p] * w[ND + p] + D.C6[p] * w[ND + NL + p];
+    const T e1 = w[ND + 2 * NL];
+    E = D.C1 * E + D.C2 * e1 + curl - t1 - t2;
+#pragma unroll
+    for (int p = 0; p < ND; ++p) st[p * sc] = D.kappa[p] * w[p] + D.beta[p] * (E + temp);
+#pragma unroll
+    for (int p = 0; p < NL; ++p) {
+        const T t0 = w[ND + p];
+        st[(ND + p) * sc] = D.alpha[p] * t0 + D.xi[p] * w[ND + NL + p] + D.gammaL[p] * (E - e1) / T(2.0) / D.dt;
+        st[(ND + NL + p) * sc] = t0;
+    }
+    st[(ND + 2 * NL) * sc] = temp;
+    return E;
+}
+
 // ---------------------------------------------------------------- gain
 // FP64 layout (reference state, unscaled): words
 //   0..2 Pa, 3..5 Pa1, 6..8 Pa2, 9..11 Pb, 12..14 Pb1, 15..17 Pb2, 18..20 E1, 21..24 N0..N3

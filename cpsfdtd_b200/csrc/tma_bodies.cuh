@@ -284,7 +284,9 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
 
 // Drude-Lorentz cell c of a grid's compacted list (Drude_Lorentz.cpp:153-227
 // in 3-D form, curl of the updated H), followed by its CPML correction.
-template <typename T, bool PML>
+// ND < 0: pole counts taken at run time from D.c (any count); ND >= 0: the
+// cell's ND Drude and NL Lorentz poles fixed at compile time, state loaded first.
+template <typename T, bool PML, int ND = -1, int NL = 0>
 __device__ __forceinline__ void dl_cell(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D, int64_t c)
 {
     const Dims &d = f.d;
@@ -314,14 +316,43 @@ __device__ __forceinline__ void dl_cell(const FieldView<T> &f, const PmlView<T> 
     const T czz = C3 * dHy_i * cEzy - C3 * dHx_j * cEzx;
     const int64_t sc = D.ncell;
     T *st = D.state + c;
-    T ex = dl_component(D.c, f.Ex[g], cxx, st, sc);
-    T ey = dl_component(D.c, f.Ey[g], cyy, st + (int64_t)D.c.stride * sc, sc);
-    T ez = dl_component(D.c, f.Ez[g], czz, st + (int64_t)2 * D.c.stride * sc, sc);
+    T ex = f.Ex[g], ey = f.Ey[g], ez = f.Ez[g];
+    if (ND >= 0) {
+        // every state word of the cell is requested before any is used
+        constexpr int W = (ND < 0 ? 0 : ND) + 2 * NL + 1;
+        constexpr int NDV = ND < 0 ? 0 : ND;
+        T w[3][W];
+#pragma unroll
+        for (int cpt = 0; cpt < 3; ++cpt)
+#pragma unroll
+            for (int q = 0; q < W; ++q) w[cpt][q] = st[((int64_t)cpt * W + q) * sc];
+        ex = dl_component_regs<T, NDV, NL>(D.c, ex, cxx, w[0], st, sc);
+        ey = dl_component_regs<T, NDV, NL>(D.c, ey, cyy, w[1], st + (int64_t)W * sc, sc);
+        ez = dl_component_regs<T, NDV, NL>(D.c, ez, czz, w[2], st + (int64_t)2 * W * sc, sc);
+    } else {
+        ex = dl_component(D.c, ex, cxx, st, sc);
+        ey = dl_component(D.c, ey, cyy, st + (int64_t)D.c.stride * sc, sc);
+        ez = dl_component(D.c, ez, czz, st + (int64_t)2 * D.c.stride * sc, sc);
+    }
     if (PML) {
         const ColPml<T> pc = col_pml_e(p, d, i, j, true);
         pml_e_cell(p, d, pc, i, j, k, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
     }
     f.Ex[g] = ex; f.Ey[g] = ey; f.Ez[g] = ez;
+}
+
+// dl_cell with the pole counts of the grid's material dispatched to a
+// compile-time form where one exists
+template <typename T, bool PML>
+__device__ __forceinline__ void dl_cell_any(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D, int64_t c)
+{
+    const int nd = D.c.nD, nl = D.c.nL;
+    if (nd == 1 && nl == 2) dl_cell<T, PML, 1, 2>(f, p, D, c);
+    else if (nd == 1 && nl == 1) dl_cell<T, PML, 1, 1>(f, p, D, c);
+    else if (nd == 1 && nl == 0) dl_cell<T, PML, 1, 0>(f, p, D, c);
+    else if (nd == 0 && nl == 1) dl_cell<T, PML, 0, 1>(f, p, D, c);
+    else if (nd == 0 && nl == 2) dl_cell<T, PML, 0, 2>(f, p, D, c);
+    else dl_cell<T, PML>(f, p, D, c);
 }
 
 }  // namespace cps
