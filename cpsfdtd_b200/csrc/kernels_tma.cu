@@ -9,7 +9,7 @@ namespace cps {
 namespace {
 
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
-__global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1) k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
+__global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 * BY)) k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
                                                     DlView<T> D, GainView<T> G, int kc, int *err)
 {
     extern __shared__ __align__(128) unsigned char sm_raw[];
