@@ -492,7 +492,7 @@ class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("jobs_done", "jobs_failed", "jobs_rejected", "jobs_cancelled",
                                           "jobs_live", "jobs_queued", "bytes_in_use", "chunks")] + \
                [(n, C.c_double) for n in ("latency_p50_ms", "latency_p99_ms", "wait_p50_ms", "wait_p99_ms",
-                                           "run_p50_ms", "cell_updates", "span_s")]
+                                           "run_p50_ms", "cell_updates", "span_s", "gpu_busy_s")]
 
 
 _BUILD_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_void_p))

@@ -71,6 +71,11 @@ bool tile_in_pml_host(const int np[6], const Dims &d, int x0, int y0, int by, in
 // (1 CPML tile, 2 Drude-Lorentz grid, 4 gain grid)
 enum { kHInt, kHPml, kE0, kNumSweep = kE0 + 8 };
 
+// members of at least this many cells fill the device by themselves: their
+// sweeps are launched per grid with the one-grid kernels, whose tensor maps
+// and views are kernel parameters (faster than the shared tile tables)
+constexpr int64_t kBigCells = 4 << 20;
+
 }  // namespace
 
 struct cps_batch {
@@ -98,6 +103,7 @@ struct cps_batch {
     int4 *d_dft = nullptr; int ndft = 0;
     int nports = 0;
     int64_t cells = 0;
+    std::vector<int> big;  // members stepped with their own sweep launches
     // graphs per chunk length
     std::map<int, std::pair<cudaGraphExec_t, int64_t>> graphs;  // executable and its kernel count
     std::map<int, int> direct;  // chunk lengths launched directly since the last rebuild
@@ -154,6 +160,7 @@ void free_tables(cps_batch *b)
     b->d_phasor = nullptr; b->nphasor = 0;
     b->d_dft = nullptr; b->ndft = 0;
     b->nports = 0;
+    b->big.clear();
 }
 
 cps_status sync_grid_streams_in(cps_batch *b)
@@ -222,7 +229,11 @@ cps_status rebuild_T(cps_batch *b)
         // sweep tiles, z outermost so that neighbouring blocks share halos
         const bool gain = B.G.on && B.G.ncell > 0, dlg = B.D.on && B.D.ncell > 0;
         const int nbx = cdiv_i(d.nx, 32), nby = cdiv_i(d.ny, by), nbz = cdiv_i(d.nz, kc);
-        for (int bz = 0; bz < nbz; ++bz)
+        // a grid that fills the device alone gets its own sweep launches (tensor
+        // maps as kernel parameters); the rest of its step stays batched
+        const bool is_big = (int64_t)d.nx * d.ny * d.nz >= kBigCells;
+        if (is_big) b->big.push_back((int)gi);
+        for (int bz = 0; bz < nbz && !is_big; ++bz)
             for (int yb = 0; yb < nby; ++yb)
                 for (int xb = 0; xb < nbx; ++xb) {
                     const int4 t = make_int4((int)gi, xb, yb, bz);
@@ -241,7 +252,7 @@ cps_status rebuild_T(cps_batch *b)
                         }
                     }
                 }
-        if (B.D.on && B.D.ncell > 0) {
+        if (B.D.on && B.D.ncell > 0 && !is_big) {
             REQUIRE(B.D.ncell < INT32_MAX, CPS_E_INVALID, "batch: Drude-Lorentz list too long");
             for (int64_t c0 = 0; c0 < B.D.ncell; c0 += 128)
                 dl.push_back(make_int4((int)gi, (int)c0, (int)std::min<int64_t>(c0 + 128, B.D.ncell), 0));
@@ -288,6 +299,7 @@ cps_status rebuild_T(cps_batch *b)
     CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
     // kernel attributes are set here, outside any stream capture
     batch_kernel_attributes<T>();
+    tma_attributes<T>();
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -335,15 +347,25 @@ int64_t enqueue_chunk(cps_batch *b, int S)
     for (int s = 0; s < S; ++s) {
         launch_h_batch<T>(G, b->d_tiles[kHInt], b->ntiles[kHInt], b->nblocks[kHInt], b->by, false, b->d_err, st);
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
+        for (int gi : b->big) {
+            const cps_grid *g = b->grids[gi];
+            launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, st);
+        }
         launch_inject_batch<T>(G, b->d_inj[1], b->ninj[1], 1, s, st);
         for (int c = 0; c < 8; ++c)
             launch_e_batch<T>(G, b->d_tiles[kE0 + c], b->ntiles[kE0 + c], b->nblocks[kE0 + c], b->by, c, b->d_err, st);
         launch_dl_batch<T>(G, b->d_dl, b->ndl, st);
+        for (int gi : b->big) {
+            const cps_grid *g = b->grids[gi];
+            launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
+                            FusedShape{b->by, b->kc}, b->d_err, st);
+        }
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);
         launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, st);
         for (int c = 0; c < kNumSweep; ++c) n += b->ntiles[c] > 0;
         n += (b->ndl > 0) + (b->ninj[0] > 0) + (b->ninj[1] > 0) + (b->nsrc > 0) + (b->ngather > 0);
+        for (int gi : b->big) n += 2 + (b->grids[gi]->dl_on && b->grids[gi]->dl_n > 0);
     }
     launch_dft_batch<T>(G, P, b->d_phasor, b->nphasor, b->d_dft, b->ndft, S, st);
     n += b->ndft > 0 ? 2 : 0;

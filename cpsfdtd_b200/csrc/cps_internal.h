@@ -178,6 +178,9 @@ void launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, 
 template <typename T>
 void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
                   const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s);
+// set the shared-memory attributes of every TMA sweep kernel (call outside captures)
+template <typename T>
+void tma_attributes();
 
 // Ports (kernels_ports.cu)
 constexpr int kMaxGather = 16;

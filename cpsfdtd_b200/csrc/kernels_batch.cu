@@ -25,11 +25,13 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap *map)
                  : "memory");
 }
 
-__device__ __forceinline__ void acquire_maps(const TmaMaps &M)
+// the seven maps one sweep side reads: E sweep H halos + E tiles + IDs, H
+// sweep E halos + H tiles + IDs
+__device__ __forceinline__ void acquire_maps(const TmaMaps &M, bool eside)
 {
-    for (int c = 0; c < 6; ++c) {
-        tensormap_acquire(&M.halo[c]);
-        tensormap_acquire(&M.own[c]);
+    for (int c = 0; c < 3; ++c) {
+        tensormap_acquire(&M.halo[eside ? 3 + c : c]);
+        tensormap_acquire(&M.own[eside ? c : 3 + c]);
     }
     tensormap_acquire(&M.id);
 }
@@ -49,7 +51,7 @@ __global__ void __launch_bounds__(32 * BY) k_h_batch(const BatchGrid<T> *__restr
         const int4 e = tiles[q];
         const BatchGrid<T> &B = grids[e.x];
         if (e.x != last) {
-            if (lead) acquire_maps(B.M);
+            if (lead) acquire_maps(B.M, false);
             last = e.x;
         }
         if (!h_tma_body<T, BY, PML>(B.M, B.f, B.p, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm, full)) return;
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restr
         const int4 e = tiles[q];
         const BatchGrid<T> &B = grids[e.x];
         if (e.x != last) {
-            if (lead) acquire_maps(B.M);
+            if (lead) acquire_maps(B.M, true);
             last = e.x;
         }
         if (!e_tma_body<T, BY, PML, DL, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm,

@@ -56,16 +56,24 @@ __global__ void __launch_bounds__(128) k_dl_cells(FieldView<T> f, PmlView<T> p, 
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// the shared-memory attribute of each kernel, set once (outside any capture
+// when tma_attributes runs first)
+template <auto K>
+void set_smem(int bytes)
+{
+    static bool done = false;
+    if (!done) {
+        cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        done = true;
+    }
+}
+
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
 void e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
                   const GainView<T> &G, int kc, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_e_tma<T, BY, PML, DL, GAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-        attr = true;
-    }
+    set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM);
     dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
     k_e_tma<T, BY, PML, DL, GAIN><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, err);
 }
@@ -74,13 +82,25 @@ template <typename T, int BY, bool PML>
 void h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_h_tma<T, BY, PML>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::SMEM);
-        attr = true;
-    }
+    set_smem<k_h_tma<T, BY, PML>>(L::SMEM);
     dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
     k_h_tma<T, BY, PML><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, err);
+}
+
+template <typename T, int BY>
+void attrs_by()
+{
+    constexpr int S = StageLayout<T, BY>::SMEM;
+    set_smem<k_h_tma<T, BY, false>>(S);
+    set_smem<k_h_tma<T, BY, true>>(S);
+    set_smem<k_e_tma<T, BY, false, false, false>>(S);
+    set_smem<k_e_tma<T, BY, false, false, true>>(S);
+    set_smem<k_e_tma<T, BY, false, true, false>>(S);
+    set_smem<k_e_tma<T, BY, false, true, true>>(S);
+    set_smem<k_e_tma<T, BY, true, false, false>>(S);
+    set_smem<k_e_tma<T, BY, true, false, true>>(S);
+    set_smem<k_e_tma<T, BY, true, true, false>>(S);
+    set_smem<k_e_tma<T, BY, true, true, true>>(S);
 }
 
 template <typename T, int BY>
@@ -128,6 +148,15 @@ void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, 
     }
 }
 
+template <typename T>
+void tma_attributes()
+{
+    attrs_by<T, 4>();
+    attrs_by<T, 8>();
+}
+
+template void tma_attributes<float>();
+template void tma_attributes<double>();
 template void launch_h_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &, FusedShape, int *,
                                   cudaStream_t);
 template void launch_h_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &, FusedShape,

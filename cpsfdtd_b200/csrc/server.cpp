@@ -44,6 +44,7 @@ cps_status cps_batch_remove(cps_batch *b, cps_grid *g);
 cps_status cps_batch_step(cps_batch *b, int32_t nsteps);
 cps_status cps_batch_synchronize(cps_batch *b);
 cps_status cps_batch_set_tile(cps_batch *b, int32_t rows, int32_t planes, int32_t persistent);
+cps_status cps_batch_get_stream(const cps_batch *b, void **stream);
 cps_status cps_grid_destroy(cps_grid *g);
 cps_status cps_grid_bytes(const cps_grid *g, int64_t *bytes);
 }
@@ -106,6 +107,8 @@ struct cps_server {
     double cell_updates = 0;
     double t_first = -1, t_last = 0;
     int64_t chunks = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the chunk in flight
+    double gpu_ms = 0;
 };
 
 namespace {
@@ -236,6 +239,9 @@ cps_status complete(cps_server *s)
 {
     if (s->inflight.empty()) return CPS_OK;
     const cps_status st = cps_batch_synchronize(s->batch);
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, s->ev0, s->ev1) == cudaSuccess) s->gpu_ms += ms;
+    else cudaGetLastError();
     for (Job *j : s->inflight) {
         j->done_steps += s->inflight_steps;
         s->cell_updates += (double)j->cells * s->inflight_steps;
@@ -262,7 +268,11 @@ cps_status launch(cps_server *s)
     int32_t S = s->cfg.chunk_steps;
     for (Job *j : s->live) S = std::min(S, j->nsteps - j->done_steps);
     if (S <= 0) return CPS_OK;
+    void *stream = nullptr;
+    cps_batch_get_stream(s->batch, &stream);
+    cudaEventRecord(s->ev0, (cudaStream_t)stream);
     const cps_status st = cps_batch_step(s->batch, S);
+    cudaEventRecord(s->ev1, (cudaStream_t)stream);
     if (st != CPS_OK) {
         for (Job *j : s->live) {
             cps_batch_remove(s->batch, j->g);
@@ -299,6 +309,8 @@ extern "C" cps_status cps_server_create(const cps_server_config *cfg, cps_server
         return st;
     }
     cudaGetDevice(&s->device);
+    cudaEventCreate(&s->ev0);
+    cudaEventCreate(&s->ev1);
     s->builder = std::thread(builder_main, s);
     *out = s;
     return CPS_OK;
@@ -398,6 +410,7 @@ extern "C" cps_status cps_server_get_stats(const cps_server *s, cps_server_stats
     out->run_p50_ms = percentile(s->run, 0.50);
     out->cell_updates = s->cell_updates;
     out->span_s = s->t_first >= 0 && s->t_last > s->t_first ? s->t_last - s->t_first : 0.0;
+    out->gpu_busy_s = s->gpu_ms / 1e3;
     return CPS_OK;
 }
 
@@ -425,6 +438,8 @@ extern "C" cps_status cps_server_destroy(cps_server *s)
         finish(s, j, CPS_E_CANCELLED);
     }
     cps_batch_destroy(s->batch);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
     delete s;
     return CPS_OK;
 }

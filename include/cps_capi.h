@@ -350,6 +350,7 @@ typedef struct cps_server_stats {
     double run_p50_ms;                       /* admitted -> done */
     double cell_updates;                     /* of all chunks completed */
     double span_s;                           /* first submit -> last finished job */
+    double gpu_busy_s;                       /* device time of the chunks (events on the batch stream) */
 } cps_server_stats;
 CPS_API cps_status cps_server_create(const cps_server_config *cfg, cps_server **out);
 CPS_API cps_status cps_server_destroy(cps_server *s);   /* cancels what is left */

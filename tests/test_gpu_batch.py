@@ -163,3 +163,23 @@ def test_batch_autotune_cache(tmp_path):
     # the tuning steps were real steps: members match grids stepped alone
     for dk, g in zip(dks, gs):
         _same(_alone(dk, cps.FP32, ran), _state(g), "autotuned")
+
+
+def test_batch_with_a_large_member_equals_alone():
+    """A member of more than 4 M cells is swept by its own launches inside the
+    batch's chunk; it and a small co-member still match their alone runs."""
+    import cpsfdtd_b200 as cps
+    steps = 70
+    big = decks.config2(n=164, steps=steps, nfreq=2)
+    small = decks.config4_member(40, 48, 36, seed=2, steps=steps, nfreq=3)
+    ref = [_alone(dk, cps.FP32, steps) for dk in (big, small)]
+    b = cps.Batch(cps.FP32)
+    gs = [_grid(dk, cps.FP32) for dk in (big, small)]
+    for g in gs:
+        b.add(g)
+    b.step(30)
+    b.step(30)
+    b.step(10)
+    b.sync()
+    for n, g in enumerate(gs):
+        _same(ref[n], _state(g), f"member {n}")
