@@ -432,6 +432,7 @@ def serving(args, local):
             "latency_p50_s": pct(lat, 50), "latency_p99_s": pct(lat, 99),
             "server_latency_p50_ms": st["latency_p50_ms"], "server_latency_p99_ms": st["latency_p99_ms"],
             "wait_p50_ms": st["wait_p50_ms"], "chunks": st["chunks"], "failed": st["jobs_failed"],
+            "gpu_busy_s": st["gpu_busy_s"],
             "budget_bytes": budget, "span_s": span,
             "plain_one_at_a_time": {"jobs_per_s": len(jobs) / max(finish, 1e-9),
                                     "gcell_upd_per_s": cells_total / sum(service) / 1e9,
