@@ -117,6 +117,8 @@ def lib():
             "cps_op_gain_efield": ([P], I32), "cps_op_gain_populations": ([P], I32),
             "cps_op_tfsf_h": ([P, I32, U32], I32), "cps_op_tfsf_e": ([P, I32, U32], I32),
             "cps_op_sources": ([P, I32], I32), "cps_op_port_sample": ([P, I32, I32], I32),
+            "cps_grid_set_record": ([P, I32], I32),
+            "cps_grid_record_stats": ([P, C.POINTER(I64), C.POINTER(I64), ip], I32),
             "cps_field_download": ([P, I32, dp], I32), "cps_field_upload": ([P, I32, dp], I32),
             "cps_field_download_f32": ([P, I32, C.POINTER(C.c_float)], I32),
             "cps_grid_reset": ([P, I64], I32), "cps_grid_check_finite": ([P, C.POINTER(I64)], I32),
@@ -323,6 +325,16 @@ class Grid:
     def op(self, name, *args):
         _check(getattr(self.L, "cps_op_" + name)(self.h, *args))
 
+    def set_record(self, on):
+        """Queue op() calls; a whole step in the reference's order runs fused."""
+        _check(self.L.cps_grid_set_record(self.h, 1 if on else 0))
+
+    def record_stats(self):
+        """(steps run fused, calls replayed one by one, calls queued now)"""
+        f, r, q = C.c_int64(), C.c_int64(), C.c_int32()
+        _check(self.L.cps_grid_record_stats(self.h, C.byref(f), C.byref(r), C.byref(q)))
+        return f.value, r.value, q.value
+
     # ------------------------------------------------------- access
     def field(self, comp):
         out = np.empty(self.shape3, dtype=np.float64)
@@ -498,7 +510,9 @@ class ServerStats(C.Structure):
 _BUILD_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_void_p))
 _DONE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32)
 
-CPS_E_INVALID, CPS_E_BUDGET, CPS_E_CANCELLED = 1, 6, 8
+# status codes of cps_capi.h
+CPS_OK, CPS_E_INVALID, CPS_E_CUDA, CPS_E_NOMEM, CPS_E_STATE = 0, 1, 2, 3, 4
+CPS_E_NUMERIC, CPS_E_BUDGET, CPS_E_TIMEOUT, CPS_E_CANCELLED, CPS_E_NOTFOUND = 5, 6, 7, 8, 9
 
 
 def footprint(dk, precision=FP32) -> int:

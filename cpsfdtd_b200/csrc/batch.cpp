@@ -610,6 +610,10 @@ extern "C" cps_status cps_batch_step(cps_batch *b, int32_t nsteps)
     REQUIRE(b, CPS_E_INVALID, "cps_batch_step: NULL batch");
     REQUIRE(nsteps >= 0, CPS_E_INVALID, "cps_batch_step: negative step count");
     if (nsteps == 0 || b->grids.empty()) return CPS_OK;
+    for (cps_grid *g : b->grids) {  // calls recorded on a member run first, on its own stream
+        cps_status s = flush_recorded(g);
+        if (s) return s;
+    }
     return b->fp32 ? step_batch_T<float>(b, nsteps) : step_batch_T<double>(b, nsteps);
 }
 

@@ -25,6 +25,13 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 
 using namespace cps;
 
+// calls recorded on the grid run before anything that reads or changes its state
+#define FLUSH_RECORDED(g)                                  \
+    do {                                                   \
+        cps_status fs_ = cps::flush_recorded(g);           \
+        if (fs_) return fs_;                               \
+    } while (0)
+
 extern "C" const char *cps_last_error(void) { return g_last_error.c_str(); }
 extern "C" const char *cps_version(void) { return "cpsfdtd-b200 0.1 (sm_100a)"; }
 
@@ -254,7 +261,7 @@ void op_sources(cps_grid *g, int n)
 // Sample ports into their rings (Update_Fields_on_Port), all ports of the
 // list in one launch; a full ring is first folded into the DFT accumulators.
 template <typename T>
-cps_status op_ports(cps_grid *g, PortState *const *ports, int nports, int64_t n)
+cps_status op_ports(cps_grid *g, PortState *const *ports, int nports, int64_t n, const int64_t *port_n = nullptr)
 {
     for (int b0 = 0; b0 < nports; b0 += kMaxGather) {
         GatherBatch B;
@@ -265,7 +272,7 @@ cps_status op_ports(cps_grid *g, PortState *const *ports, int nports, int64_t n)
                 cps_status s = flush_dft(g, P);
                 if (s) return s;
             }
-            if (P.fill == 0) P.ring_n0 = n;
+            if (P.fill == 0) P.ring_n0 = port_n ? port_n[q] : n;
             GatherDesc &D = B.p[B.n++];
             D.idx = P.d_idx;
             D.slot = (T *)P.d_ring + (int64_t)P.fill * 6 * P.npts;
@@ -567,6 +574,7 @@ extern "C" cps_status cps_grid_bytes(const cps_grid *g, int64_t *bytes)
 extern "C" cps_status cps_grid_set_stream(cps_grid *g, void *stream)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    FLUSH_RECORDED(g);
     CK(cudaStreamSynchronize(g->stream));
     if (g->own_stream && stream) { cudaStreamDestroy(g->stream); g->own_stream = false; }
     if (stream) g->stream = (cudaStream_t)stream;
@@ -583,6 +591,7 @@ extern "C" cps_status cps_grid_get_stream(const cps_grid *g, void **stream)
 extern "C" cps_status cps_synchronize(cps_grid *g)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    FLUSH_RECORDED(g);
     CK(cudaStreamSynchronize(g->stream));
     return check_device_error(g);
 }
@@ -593,6 +602,7 @@ extern "C" cps_status cps_grid_set_media(cps_grid *g, int32_t n, const double *e
                                          const double *sig, const double *sigM)
 {
     REQUIRE(g && epsR && muR && sig && sigM, CPS_E_INVALID, "cps_grid_set_media: NULL argument");
+    FLUSH_RECORDED(g);
     REQUIRE(n >= 1 && n <= 256, CPS_E_INVALID, "cps_grid_set_media: 1..256 media");
     const double dt = g->desc.dt;
     for (int i = 0; i < n; ++i) {
@@ -612,6 +622,7 @@ extern "C" cps_status cps_grid_set_media(cps_grid *g, int32_t n, const double *e
 extern "C" cps_status cps_grid_upload_ids(cps_grid *g, const uint8_t *ids)
 {
     REQUIRE(g && ids, CPS_E_INVALID, "cps_grid_upload_ids: NULL argument");
+    FLUSH_RECORDED(g);
     REQUIRE(!g->dl_on && !g->gain_on && !g->pml_on, CPS_E_STATE,
             "cps_grid_upload_ids: IDs must be set before the physics modules are initialised");
     const Dims &d = g->d;
@@ -650,6 +661,7 @@ extern "C" cps_status cps_pml_init(cps_grid *g, const cps_pml_params *pp)
 {
     cps_status s = need_setup(g);
     if (s) return s;
+    FLUSH_RECORDED(g);
     REQUIRE(pp, CPS_E_INVALID, "cps_pml_init: NULL params");
     REQUIRE(!g->pml_on, CPS_E_STATE, "cps_pml_init: CPML already initialised");
     const int nax[3] = {g->d.nx, g->d.ny, g->d.nz};
@@ -721,6 +733,7 @@ extern "C" cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p)
 {
     cps_status s = need_setup(g);
     if (s) return s;
+    FLUSH_RECORDED(g);
     REQUIRE(p, CPS_E_INVALID, "cps_dl_init: NULL params");
     REQUIRE(!g->dl_on, CPS_E_STATE, "cps_dl_init: already initialised");
     REQUIRE(p->nD >= 0 && p->nL >= 0 && p->nD <= kMaxPoles && p->nL <= kMaxPoles && p->nD + p->nL > 0,
@@ -768,6 +781,7 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
 {
     cps_status s = need_setup(g);
     if (s) return s;
+    FLUSH_RECORDED(g);
     REQUIRE(p, CPS_E_INVALID, "cps_gain_init: NULL params");
     REQUIRE(!g->gain_on, CPS_E_STATE, "cps_gain_init: already initialised");
     REQUIRE(p->gain_id >= 0 && p->gain_id < 256 && p->gain_id != CPS_ID_DISPERSIVE && p->gain_id != CPS_ID_PEC,
@@ -831,6 +845,7 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
 {
     cps_status s = need_setup(g);
     if (s) return s;
+    FLUSH_RECORDED(g);
     REQUIRE(p, CPS_E_INVALID, "cps_tfsf_init: NULL params");
     REQUIRE(!g->tfsf_on, CPS_E_STATE, "cps_tfsf_init: already initialised");
     const Dims &d = g->d;
@@ -990,6 +1005,7 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
 extern "C" cps_status cps_tfsf_set_tables(cps_grid *g, int32_t n, const double *einc, const double *hinc)
 {
     REQUIRE(g && einc && hinc, CPS_E_INVALID, "NULL argument");
+    FLUSH_RECORDED(g);
     REQUIRE(g->tfsf_on, CPS_E_STATE, "TF/SF is not initialised");
     REQUIRE(n == g->tp.Nt + 1, CPS_E_INVALID, "tables must hold Nt + 1 values");
     g->einc.assign(einc, einc + n);
@@ -1011,6 +1027,7 @@ extern "C" cps_status cps_source_add(cps_grid *g, int32_t comp, int32_t i, int32
                                      int32_t nwave)
 {
     REQUIRE(g && wave, CPS_E_INVALID, "cps_source_add: NULL argument");
+    FLUSH_RECORDED(g);
     REQUIRE(comp >= 0 && comp < 6 && nwave >= 1, CPS_E_INVALID, "cps_source_add: bad component or wave length");
     REQUIRE(i >= 0 && j >= 0 && k >= 0 && i <= g->d.nx && j <= g->d.ny && k <= g->d.nz, CPS_E_INVALID,
             "cps_source_add: point outside the grid");
@@ -1052,6 +1069,7 @@ extern "C" cps_status cps_port_set_dft(cps_grid *g, int32_t port_id, int32_t nfr
 {
     REQUIRE(g && freq_hz, CPS_E_INVALID, "cps_port_set_dft: NULL argument");
     REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_set_dft: no such port");
+    FLUSH_RECORDED(g);
     REQUIRE(nfreq >= 1 && nfreq <= 4096 && (comp_mask & 63u), CPS_E_INVALID, "cps_port_set_dft: 1..4096 frequencies and a component");
     PortState &P = g->ports[port_id];
     REQUIRE(P.nfreq == 0, CPS_E_STATE, "cps_port_set_dft: DFT already configured");
@@ -1096,6 +1114,7 @@ extern "C" cps_status cps_port_read(cps_grid *g, int32_t port_id, double *out)
 {
     REQUIRE(g && out, CPS_E_INVALID, "cps_port_read: NULL argument");
     REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_read: no such port");
+    FLUSH_RECORDED(g);
     PortState &P = g->ports[port_id];
     return g->fp32 ? port_read_T<float>(g, P, out) : port_read_T<double>(g, P, out);
 }
@@ -1104,6 +1123,7 @@ extern "C" cps_status cps_port_dft_read(cps_grid *g, int32_t port_id, double *ou
 {
     REQUIRE(g && out, CPS_E_INVALID, "cps_port_dft_read: NULL argument");
     REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_dft_read: no such port");
+    FLUSH_RECORDED(g);
     PortState &P = g->ports[port_id];
     REQUIRE(P.nfreq > 0, CPS_E_STATE, "cps_port_dft_read: no DFT configured on this port");
     cps_status s = flush_dft(g, P);
@@ -1118,6 +1138,7 @@ extern "C" cps_status cps_port_flux(cps_grid *g, int32_t port_id, char normal, d
 {
     REQUIRE(g && out, CPS_E_INVALID, "cps_port_flux: NULL argument");
     REQUIRE(port_id >= 0 && port_id < (int)g->ports.size(), CPS_E_NOTFOUND, "cps_port_flux: no such port");
+    FLUSH_RECORDED(g);
     PortState &P = g->ports[port_id];
     REQUIRE(P.nfreq > 0, CPS_E_STATE, "cps_port_flux: no DFT configured on this port");
     int a, b, c, e;  // flux = Re(E_a H_b* - E_c H_e*)
@@ -1166,70 +1187,275 @@ extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
 {
     cps_status s = need_setup(g);
     if (s) return s;
+    FLUSH_RECORDED(g);
     REQUIRE(nsteps >= 0, CPS_E_INVALID, "cps_step: negative step count");
     REQUIRE(path == CPS_PATH_PLAIN || path == CPS_PATH_FUSED, CPS_E_INVALID, "cps_step: unknown path");
     CK(cudaSetDevice(g->desc.device));
     return g->fp32 ? step_T<float>(g, nsteps, path) : step_T<double>(g, nsteps, path);
 }
 
-#define OP_BODY(stmt)                                                                              \
-    cps_status s = need_setup(g);                                                                  \
-    if (s) return s;                                                                               \
-    if (g->fp32) { using T = float; stmt; } else { using T = double; stmt; }                       \
-    g->launches++;                                                                                 \
-    return cudaGetLastError() == cudaSuccess ? CPS_OK : (set_error("kernel launch failed"), CPS_E_CUDA);
+// ============================================================ op recorder
+//
+// The reference's main loop calls one routine per physics term each step
+// (main.cpp:264-330).  Each cps_op_* entry point runs that routine alone; with
+// recording on (cps_grid_set_record) the calls are queued instead, and a queue
+// that forms one whole step in an order the fused sweeps reproduce runs as one
+// fused H sweep and one fused E sweep.  The order rules: H_BULK first; TF/SF-H
+// and H_PML (additive to H) in any order before E_BULK; DL, then gain P, E, N,
+// after E_BULK; TF/SF-E, sources and E_PML (additive to E) in any order after
+// the dispersive terms; port samples last, each port once.  The terms the
+// sweeps absorb (PML, DL, gain) appear exactly once when initialised; TF/SF and
+// sources run as recorded, with their own step index, face mask and count.
+// Anything else is replayed call by call, in order.
 
-extern "C" cps_status cps_op_h_bulk(cps_grid *g) { OP_BODY(launch_h_bulk<T>(field_view<T>(g), g->stream)) }
-extern "C" cps_status cps_op_e_bulk(cps_grid *g) { OP_BODY(launch_e_bulk<T>(field_view<T>(g), g->stream)) }
+namespace cps {
+namespace {
+
+bool absorbed_kind(int k) { return k == kOpHPml || k == kOpEPml || k == kOpDl || (k >= kOpGainP && k <= kOpGainN); }
+
+// Whether `ops` is a prefix (full = false) or a whole step (full = true) that
+// the fused sweeps reproduce.
+bool fusable(const cps_grid *g, const std::vector<RecOp> &ops, bool full)
+{
+    int phase = 0;  // 0 start, 1 H terms, 2 dispersive E terms, 3 additive E terms, 4 ports
+    int hpml = 0, epml = 0, dl = 0, gain = 0;
+    std::vector<char> seen(g->ports.size(), 0);
+    const int want_dl = g->dl_on ? 1 : 0, want_gain = g->gain_on ? 3 : 0;
+    for (const RecOp &o : ops) {
+        switch (o.kind) {
+        case kOpHBulk:
+            if (phase != 0) return false;
+            phase = 1;
+            break;
+        case kOpHPml:
+            if (phase != 1 || hpml++) return false;
+            break;
+        case kOpTfsfH:
+            if (phase != 1) return false;
+            break;
+        case kOpEBulk:
+            if (phase != 1) return false;
+            phase = 2;
+            break;
+        case kOpDl:
+            if (phase != 2 || dl++ || gain) return false;
+            break;
+        case kOpGainP:
+        case kOpGainE:
+        case kOpGainN:
+            if (phase != 2 || gain != o.kind - kOpGainP) return false;
+            ++gain;
+            break;
+        case kOpTfsfE:
+        case kOpSrc:
+        case kOpEPml:
+            if (phase == 2) {
+                if (dl != want_dl || gain != want_gain) return false;
+                phase = 3;
+            }
+            if (phase != 3) return false;
+            if (o.kind == kOpEPml && epml++) return false;
+            break;
+        case kOpPort:
+            if (phase < 2) return false;
+            if (phase == 2 && (dl != want_dl || gain != want_gain)) return false;
+            phase = 4;
+            if (seen[o.port]++) return false;
+            break;
+        default:
+            return false;
+        }
+    }
+    if (!full) return true;
+    const int want_pml = g->pml_on ? 1 : 0;
+    return phase >= 2 && hpml == want_pml && epml == want_pml && dl == want_dl && gain == want_gain;
+}
+
+// one routine alone on the grid's stream
+template <typename T>
+cps_status run_op_T(cps_grid *g, const RecOp &o)
+{
+    const FieldView<T> f = field_view<T>(g);
+    switch (o.kind) {
+    case kOpHBulk: launch_h_bulk<T>(f, g->stream); g->launches++; break;
+    case kOpEBulk: launch_e_bulk<T>(f, g->stream); g->launches++; break;
+    case kOpHPml: launch_h_pml<T>(f, pml_view<T>(g), g->stream); g->launches++; break;
+    case kOpEPml: launch_e_pml<T>(f, pml_view<T>(g), g->stream); g->launches++; break;
+    case kOpDl: launch_dl<T>(f, dl_view<T>(g), g->stream); g->launches++; break;
+    case kOpGainP:
+    case kOpGainE:
+    case kOpGainN: launch_gain<T>(f, gain_view<T>(g), o.kind - kOpGainP, g->stream); g->launches++; break;
+    case kOpTfsfH: op_inject<T>(g, 1, (double)o.n, o.mask); break;
+    case kOpTfsfE: op_inject<T>(g, 0, (double)o.n, o.mask); break;
+    case kOpSrc: {
+        cps_status s = ensure_sources(g);
+        if (s) return s;
+        op_sources<T>(g, o.n);
+        break;
+    }
+    case kOpPort: {
+        cps_status s = op_port<T>(g, g->ports[o.port], o.n);
+        if (s) return s;
+        break;
+    }
+    default: break;
+    }
+    cudaError_t e = cudaGetLastError();
+    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+    return CPS_OK;
+}
+
+// one whole recorded step as the fused H and E sweeps (the step of step_T's
+// fused path, with the recorded TF/SF, source and port calls)
+template <typename T>
+cps_status run_fused_T(cps_grid *g, const std::vector<RecOp> &ops)
+{
+    cps_status s = ensure_sources(g);
+    if (s) return s;
+    const bool use_tma = g->sweep_mode == 0 && (g->shape.by == 4 || g->shape.by == 8) && g->d.px >= 64 &&
+                         g->d.ny + 1 >= g->shape.by + 1;
+    if (use_tma && (s = ensure_tma(g))) return s;
+    const FieldView<T> f = field_view<T>(g);
+    const PmlView<T> p = pml_view<T>(g);
+    std::vector<PortState *> ports;
+    std::vector<int64_t> port_n;
+    for (const RecOp &o : ops) {
+        switch (o.kind) {
+        case kOpHBulk:
+            if (use_tma) launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
+            else launch_h_fused<T>(f, p, g->shape, g->stream);
+            g->launches++;
+            break;
+        case kOpEBulk:
+            if (use_tma) launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream);
+            else launch_e_fused<T>(f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->stream);
+            g->launches++;
+            break;
+        case kOpTfsfH: op_inject<T>(g, 1, (double)o.n, o.mask); break;
+        case kOpTfsfE: op_inject<T>(g, 0, (double)o.n, o.mask); break;
+        case kOpSrc: op_sources<T>(g, o.n); break;
+        case kOpPort:
+            ports.push_back(&g->ports[o.port]);
+            port_n.push_back(o.n);
+            break;
+        default: break;  // absorbed by the sweeps
+        }
+    }
+    if (!ports.empty() && (s = op_ports<T>(g, ports.data(), (int)ports.size(), 0, port_n.data()))) return s;
+    cudaError_t e = cudaGetLastError();
+    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("kernel launch failed: ") + cudaGetErrorString(e));
+    return CPS_OK;
+}
+
+// queue one call; a call that cannot continue a fusable step flushes the queue
+cps_status record_op(cps_grid *g, const RecOp &o)
+{
+    if (o.kind == kOpHBulk && !g->pending.empty()) {
+        cps_status s = flush_recorded(g);
+        if (s) return s;
+    }
+    g->pending.push_back(o);
+    return fusable(g, g->pending, false) ? CPS_OK : flush_recorded(g);
+}
+
+cps_status submit_op(cps_grid *g, const RecOp &o)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    if (g->record) return record_op(g, o);
+    return g->fp32 ? run_op_T<float>(g, o) : run_op_T<double>(g, o);
+}
+
+}  // namespace
+
+cps_status flush_recorded(cps_grid *g)
+{
+    if (g->pending.empty()) return CPS_OK;
+    std::vector<RecOp> ops;
+    ops.swap(g->pending);
+    if (fusable(g, ops, true)) {
+        g->fused_steps++;
+        return g->fp32 ? run_fused_T<float>(g, ops) : run_fused_T<double>(g, ops);
+    }
+    for (const RecOp &o : ops) {
+        g->replayed_ops++;
+        cps_status s = g->fp32 ? run_op_T<float>(g, o) : run_op_T<double>(g, o);
+        if (s) return s;
+    }
+    return CPS_OK;
+}
+
+}  // namespace cps
+
+extern "C" cps_status cps_grid_set_record(cps_grid *g, int32_t on)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    if (!on) {
+        cps_status s = flush_recorded(g);
+        g->record = false;
+        return s;
+    }
+    g->record = true;
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_record_stats(const cps_grid *g, int64_t *fused_steps, int64_t *replayed_calls,
+                                            int32_t *pending)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    if (fused_steps) *fused_steps = g->fused_steps;
+    if (replayed_calls) *replayed_calls = g->replayed_ops;
+    if (pending) *pending = (int32_t)g->pending.size();
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_op_h_bulk(cps_grid *g) { return submit_op(g, {kOpHBulk, 0, 0, 0}); }
+extern "C" cps_status cps_op_e_bulk(cps_grid *g) { return submit_op(g, {kOpEBulk, 0, 0, 0}); }
 extern "C" cps_status cps_op_h_pml(cps_grid *g)
 {
     if (g && !g->pml_on) { set_error("CPML not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_h_pml<T>(field_view<T>(g), pml_view<T>(g), g->stream))
+    return submit_op(g, {kOpHPml, 0, 0, 0});
 }
 extern "C" cps_status cps_op_e_pml(cps_grid *g)
 {
     if (g && !g->pml_on) { set_error("CPML not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_e_pml<T>(field_view<T>(g), pml_view<T>(g), g->stream))
+    return submit_op(g, {kOpEPml, 0, 0, 0});
 }
 extern "C" cps_status cps_op_dl(cps_grid *g)
 {
     if (g && !g->dl_on) { set_error("Drude-Lorentz not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_dl<T>(field_view<T>(g), dl_view<T>(g), g->stream))
+    return submit_op(g, {kOpDl, 0, 0, 0});
 }
 extern "C" cps_status cps_op_gain_polarization(cps_grid *g)
 {
     if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 0, g->stream))
+    return submit_op(g, {kOpGainP, 0, 0, 0});
 }
 extern "C" cps_status cps_op_gain_efield(cps_grid *g)
 {
     if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 1, g->stream))
+    return submit_op(g, {kOpGainE, 0, 0, 0});
 }
 extern "C" cps_status cps_op_gain_populations(cps_grid *g)
 {
     if (g && !g->gain_on) { set_error("gain not initialised"); return CPS_E_STATE; }
-    OP_BODY(launch_gain<T>(field_view<T>(g), gain_view<T>(g), 2, g->stream))
+    return submit_op(g, {kOpGainN, 0, 0, 0});
 }
 extern "C" cps_status cps_op_tfsf_h(cps_grid *g, int32_t n, uint32_t face_mask)
 {
     if (g && !g->tfsf_on) { set_error("TF/SF not initialised"); return CPS_E_STATE; }
-    OP_BODY(op_inject<T>(g, 1, (double)n, face_mask))
+    return submit_op(g, {kOpTfsfH, n, 0, face_mask});
 }
 extern "C" cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask)
 {
     if (g && !g->tfsf_on) { set_error("TF/SF not initialised"); return CPS_E_STATE; }
-    OP_BODY(op_inject<T>(g, 0, (double)n, face_mask))
+    return submit_op(g, {kOpTfsfE, n, 0, face_mask});
 }
-extern "C" cps_status cps_op_sources(cps_grid *g, int32_t n)
-{
-    if (g) { cps_status s0 = ensure_sources(g); if (s0) return s0; }
-    OP_BODY(op_sources<T>(g, n))
-}
+extern "C" cps_status cps_op_sources(cps_grid *g, int32_t n) { return submit_op(g, {kOpSrc, n, 0, 0}); }
 extern "C" cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n)
 {
     if (g && (port_id < 0 || port_id >= (int)g->ports.size())) { set_error("no such port"); return CPS_E_NOTFOUND; }
-    OP_BODY(if (op_port<T>(g, g->ports[port_id], n)) return CPS_E_CUDA)
+    return submit_op(g, {kOpPort, n, port_id, 0});
 }
 
 // ============================================================ field access
@@ -1267,6 +1493,7 @@ extern "C" cps_status cps_field_download(cps_grid *g, int32_t comp, double *out)
 {
     REQUIRE(g && out, CPS_E_INVALID, "cps_field_download: NULL argument");
     REQUIRE(comp >= 0 && comp < 6, CPS_E_INVALID, "cps_field_download: component 0..5");
+    FLUSH_RECORDED(g);
     return g->fp32 ? download_T<float>(g, comp, out) : download_T<double>(g, comp, out);
 }
 
@@ -1274,6 +1501,7 @@ extern "C" cps_status cps_field_upload(cps_grid *g, int32_t comp, const double *
 {
     REQUIRE(g && in, CPS_E_INVALID, "cps_field_upload: NULL argument");
     REQUIRE(comp >= 0 && comp < 6, CPS_E_INVALID, "cps_field_upload: component 0..5");
+    FLUSH_RECORDED(g);
     return g->fp32 ? upload_field_T<float>(g, comp, in) : upload_field_T<double>(g, comp, in);
 }
 
@@ -1292,6 +1520,7 @@ extern "C" cps_status cps_field_download_f32(cps_grid *g, int32_t comp, float *o
 extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    FLUSH_RECORDED(g);
     for (int c = 0; c < 6; ++c) CK(cudaMemsetAsync(g->F[c], 0, (size_t)g->elems * g->esz, g->stream));
     if (g->pml_on) {
         const Dims &d = g->d;
@@ -1323,6 +1552,7 @@ extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
 extern "C" cps_status cps_grid_check_finite(cps_grid *g, int64_t *nonfinite)
 {
     REQUIRE(g && nonfinite, CPS_E_INVALID, "NULL argument");
+    FLUSH_RECORDED(g);
     CK(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned long long), g->stream));
     if (g->fp32) launch_count_nonfinite<float>(field_view<float>(g), g->d_counter, g->stream);
     else launch_count_nonfinite<double>(field_view<double>(g), g->d_counter, g->stream);
@@ -1338,6 +1568,7 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
 {
     REQUIRE(g && ncells, CPS_E_INVALID, "NULL argument");
     REQUIRE(g->gain_on, CPS_E_STATE, "gain not initialised");
+    FLUSH_RECORDED(g);
     *ncells = g->g_n;
     if (!out) return CPS_OK;
     const int nw = g->fp32 ? kG32Words : kG64Words;
@@ -1388,6 +1619,7 @@ extern "C" cps_status cps_grid_launch_count(const cps_grid *g, int64_t *launches
 extern "C" cps_status cps_ports_flush(cps_grid *g)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    FLUSH_RECORDED(g);
     for (PortState &P : g->ports) {
         cps_status s = flush_dft(g, P);
         if (s) return s;

@@ -47,6 +47,16 @@ struct PortState {
     double *d_acc = nullptr;  // [ncomp][nfreq][2][npts]
 };
 
+// one recorded per-routine call (cps_op_*), kept until the recorder flushes
+enum RecKind { kOpHBulk, kOpEBulk, kOpHPml, kOpEPml, kOpDl, kOpGainP, kOpGainE, kOpGainN, kOpTfsfH, kOpTfsfE,
+               kOpSrc, kOpPort };
+struct RecOp {
+    int kind;
+    int32_t n;      // step index (TF/SF, sources, ports)
+    int32_t port;   // port id
+    uint32_t mask;  // TF/SF face mask
+};
+
 struct Src {
     int comp;
     int64_t idx;
@@ -138,6 +148,10 @@ struct cps_grid {
     std::vector<cudaEvent_t> ev;
     int ev_used = 0;
     std::vector<std::pair<void *, size_t>> owned;  // every device allocation and its size
+    // op recorder (cps_grid_set_record)
+    bool record = false;
+    std::vector<cps::RecOp> pending;
+    int64_t fused_steps = 0, replayed_ops = 0;
 };
 
 
@@ -151,6 +165,8 @@ cps_status ensure_sources(cps_grid *g);
 cps_status ensure_tma(cps_grid *g);
 cps_status flush_dft(cps_grid *g, PortState &P);
 cps_status check_device_error(cps_grid *g);
+// run the recorded calls of the grid (fused into one step when they form one)
+cps_status flush_recorded(cps_grid *g);
 
 inline int kStretchLen(const cps_grid *g, int w)
 {

@@ -87,6 +87,9 @@ using namespace cps;
 extern "C" cps_status cps_ports_flush_static(cps_grid *g)
 {
     REQUIRE(g, CPS_E_INVALID, "cps_ports_flush_static: NULL grid");
+    // running recorded calls may allocate (a full ring's fold, first source upload)
+    REQUIRE(g->pending.empty(), CPS_E_STATE,
+            "cps_ports_flush_static: the grid holds recorded calls not yet run (cps_synchronize first)");
     for (const PortState &P : g->ports)
         REQUIRE(P.nfreq <= kStaticMaxFreq && P.slots <= kStaticMaxSlots, CPS_E_INVALID,
                 "cps_ports_flush_static: a port has more than 256 DFT frequencies (use cps_ports_flush)");

@@ -39,6 +39,8 @@
  *                               (TF_SF.cpp:1201-1410, 988-1199)
  *   cps_op_port_sample ........ SphericalPort/PlainPort::Update_Fields_on_Port (Ports.cpp:88-99, 342-353)
  *   cps_step .................. one pass of the loop body of main.cpp:267-344
+ *   cps_grid_set_record ....... (no counterpart) runs a step's cps_op_* calls, made in
+ *                               main.cpp's order, as one fused step
  *   cps_field_download/upload . direct access to Field::Ex..Hz (Fields.h:28-33)
  *   cps_port_read ............. Port_Points::Ex..Hz after Update_Fields_on_Port
  *   cps_port_dft_read / flux .. (no reference counterpart: running FP64 DFT of the port samples)
@@ -240,6 +242,25 @@ CPS_API cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask);
 CPS_API cps_status cps_op_sources(cps_grid *g, int32_t n);
 CPS_API cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n);
 
+/* Record-and-fuse for the calls above (main.cpp:264-330 calls one routine per
+ * term each step).  With recording on, cps_op_* calls are validated and queued;
+ * a queue that forms one whole step runs as the fused H and E sweeps
+ * (CPS_PATH_FUSED's kernels) plus the recorded TF/SF, source and port calls,
+ * and any other queue is replayed call by call in its order.  Fusable order:
+ * h_bulk first; tfsf_h and h_pml in any order before e_bulk; dl, then gain
+ * polarization, efield, populations; then tfsf_e, sources and e_pml in any
+ * order; port samples last, each port at most once.  h_pml/e_pml, dl and the
+ * gain calls appear exactly once when their module is initialised.  The queue
+ * runs at the next h_bulk, at any call that reads or changes the grid (field,
+ * port, population reads, cps_synchronize, cps_step, set-up calls,
+ * cps_batch_step of a batch holding the grid) and when recording is switched
+ * off; a launch error of a recorded call is returned by the call that ran it.
+ * Off by default. */
+CPS_API cps_status cps_grid_set_record(cps_grid *g, int32_t on);
+/* steps run fused, calls replayed one by one, calls queued now; NULL skips */
+CPS_API cps_status cps_grid_record_stats(const cps_grid *g, int64_t *fused_steps, int64_t *replayed_calls,
+                                         int32_t *pending);
+
 /* ---- field access ---- */
 CPS_API cps_status cps_field_download(cps_grid *g, int32_t comp, double *out);
 CPS_API cps_status cps_field_upload(cps_grid *g, int32_t comp, const double *in);
@@ -275,7 +296,9 @@ CPS_API cps_status cps_grid_timing(cps_grid *g, double *h_sweep_ms, double *e_sw
  * all grids of a device, so ports may have at most 256 frequencies and calls
  * on one device must not overlap.  For callers that cannot allocate (a fixed
  * admitted memory budget, or a loop that must not enter the allocator).  The
- * first call on a device looks up the array's address. */
+ * first call on a device looks up the array's address.  A grid holding
+ * recorded calls not yet run (cps_grid_set_record) is refused with
+ * CPS_E_STATE: running them may allocate. */
 CPS_API cps_status cps_ports_flush_static(cps_grid *g);
 /* host FP64 copies of the per-medium coefficients (Structure::aE, bE, aH,
  * bH, Structure.cpp:309-359), NoMedia entries each; NULL skips an array */

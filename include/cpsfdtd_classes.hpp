@@ -7,8 +7,10 @@
 // Fields.h, BasicFDTD.h, CPML.h, CFS_PML.h, Drude_Lorentz.h,
 // FourLevelLaser.h, TF_SF.h and Ports.h, and links with -lcpsfdtd.
 //
-// State lives on the GPU; each update call enqueues that routine's kernels on
-// the grid's stream in call order.  The Field members Ex..Hz are host mirrors
+// State lives on the GPU; update calls are recorded on the grid
+// (cps_grid_set_record): a step made in main.cpp's order runs as the two
+// fused sweeps, any other order routine by routine, on the grid's stream in
+// call order.  CPSFDTD_RECORD=0 in the environment runs every call at once.  The Field members Ex..Hz are host mirrors
 // in the reference's [i][j][k] layout: Field::sync_to_host() fills them from
 // the device and Field::sync_to_device() writes them back (the reference
 // reads and writes them directly; here the copies are explicit).
@@ -179,6 +181,8 @@ public:
         if (!grid_) {
             cps_grid_desc d{Nx, Ny, Nz, dx, dy, dz, dt, precision_, 0};
             cpsfdtd_detail::check(cps_grid_create(&d, &grid_), "Structure grid");
+            const char *rec = getenv("CPSFDTD_RECORD");
+            cpsfdtd_detail::check(cps_grid_set_record(grid_, !(rec && strcmp(rec, "0") == 0)), "record");
         }
         cpsfdtd_detail::check(cps_grid_set_media(grid_, NoMedia, epsR, muR, sig, sigM), "media");
         upload_ids();

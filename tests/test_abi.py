@@ -52,3 +52,20 @@ def test_grid_create_without_device_fails_loudly():
     import cpsfdtd_b200 as cps
     with pytest.raises(cps.CpsError):
         cps.Grid(8, 8, 8, 1e-8, 1e-8, 1e-8)
+
+
+def test_python_status_codes_match_the_header():
+    import cpsfdtd_b200 as cps
+    text = open(os.path.join(ROOT, "include", "cps_capi.h")).read()
+    codes = dict(re.findall(r"\b(CPS_(?:OK|E_\w+))\s*=\s*(\d+)", text))
+    assert len(codes) == 10
+    for name, v in codes.items():
+        assert getattr(cps, name) == int(v), name
+
+
+def test_recorder_entry_points_validate_without_a_device():
+    import cpsfdtd_b200 as cps
+    L = cps.lib()
+    assert L.cps_grid_set_record(None, 1) == cps.CPS_E_INVALID
+    assert L.cps_grid_record_stats(None, None, None, None) == cps.CPS_E_INVALID
+    assert L.cps_op_h_bulk(None) == cps.CPS_E_INVALID

@@ -34,8 +34,11 @@ def test_dropin_main_builds_and_fails_loudly(tmp_path):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("record", ["1", "0"])
 @pytest.mark.parametrize("case", ["dispersive", "dielectric"])
-def test_dropin_matches_oracle(tmp_path, oracle_mod, case):
+def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
+    """record "1": the classes' calls run as fused steps (the default);
+    "0": routine by routine."""
     import cpsfdtd_b200 as cps
     exe = _build(tmp_path)
     if case == "dispersive":
@@ -49,7 +52,8 @@ def test_dropin_matches_oracle(tmp_path, oracle_mod, case):
     os.makedirs(out)
     dk.write(str(deck))
     nsteps = 40
-    r = subprocess.run([exe, str(deck), str(nsteps), str(out)], capture_output=True, text=True, timeout=300)
+    env = dict(os.environ, CPSFDTD_RECORD=record)
+    r = subprocess.run([exe, str(deck), str(nsteps), str(out)], capture_output=True, text=True, timeout=300, env=env)
     assert r.returncode == 0, r.stderr
     assert r.stdout.startswith("dropin ok")
 
