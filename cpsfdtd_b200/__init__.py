@@ -20,13 +20,13 @@ from .decks import ID_DISPERSIVE
 
 import numpy as np
 
-__all__ = ["Grid", "Batch", "Server", "footprint", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "LIB_PATH"]
+__all__ = ["Grid", "Batch", "Server", "footprint", "CpsError", "lib", "FP64", "FP32", "PLAIN", "FUSED", "ONEPASS", "LIB_PATH"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libcpsfdtd.so")
 
 FP64, FP32 = 0, 1
-PLAIN, FUSED = 0, 1
+PLAIN, FUSED, ONEPASS = 0, 1, 2
 MAX_POLES = 8
 
 _lib = None

@@ -33,6 +33,7 @@ SOURCES = {
     "kernels_tma.cu": [],
     "kernels_ports.cu": [],
     "kernels_batch.cu": [],
+    "kernels_step.cu": [],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
     "noalloc.cu": [],

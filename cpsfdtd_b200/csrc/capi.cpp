@@ -373,6 +373,145 @@ cps_status ensure_tma(cps_grid *g)
     return CPS_OK;
 }
 
+// tensor maps of the one-pass sweep over one buffer set (E boxes 40 x (by+2),
+// H boxes 36 x (by+1), ID box 48 x (by+1))
+cps_status encode_step_maps(cps_grid *g, void *const F[6], StepMaps *m, int by)
+{
+    EncodeTiled enc = encode_fn();
+    REQUIRE(enc, CPS_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const Dims &d = g->d;
+    const cuuint64_t dims[3] = {(cuuint64_t)d.px, (cuuint64_t)(d.ny + 1), (cuuint64_t)(d.nz + 1)};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUtensorMapDataType dt = g->fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t st[2] = {(cuuint64_t)d.px * g->esz, (cuuint64_t)d.pxy * g->esz};
+    const cuuint32_t ebox[3] = {40, (cuuint32_t)by + 2, 1}, hbox[3] = {36, (cuuint32_t)by + 1, 1};
+    const cuuint32_t ibox[3] = {48, (cuuint32_t)by + 1, 1};
+    for (int c = 0; c < 3; ++c) {
+        CUresult r1 = enc(&m->e[c], dt, 3, F[c], dims, st, ebox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        CUresult r2 = enc(&m->h[c], dt, 3, F[3 + c], dims, st, hbox, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        REQUIRE(r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for a field");
+    }
+    const cuuint64_t sid[2] = {(cuuint64_t)d.px, (cuuint64_t)d.pxy};
+    CUresult r = enc(&m->id, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, g->d_id, dims, sid, ibox, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    REQUIRE(r == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for the IDs");
+    return CPS_OK;
+}
+
+cps_status ensure_onepass(cps_grid *g)
+{
+    cps_status s;
+    if (!g->F2[0]) {
+        // zeroed once: the sweep writes every cell of the arrays, never the x padding
+        for (int c = 0; c < 6; ++c) {
+            if ((s = dalloc(g, &g->F2[c], (size_t)g->elems * g->esz))) return s;
+            CK(cudaMemsetAsync(g->F2[c], 0, (size_t)g->elems * g->esz, g->stream));
+        }
+    }
+    if (g->pml_on && !g->d_q2[0][0]) {
+        for (int f = 0; f < 6; ++f)
+            for (int q = 0; q < 2; ++q) {
+                const size_t n = psi_words(g, f) * g->esz;
+                if ((s = dalloc(g, &g->d_q2[f][q], n))) return s;
+                CK(cudaMemsetAsync(g->d_q2[f][q], 0, n, g->stream));
+            }
+    }
+    if (g->tfsf_on && g->ntg[1] > 0 && !g->d_hslot && g->hc_ok) {
+        // each H-side contribution's slot in the per-face arrays of the targets' bounding box
+        const Dims &d = g->d;
+        std::vector<InjTarget> tg(g->ntg[1]);
+        CK(cudaMemcpyAsync(tg.data(), g->d_tg[1], tg.size() * sizeof(InjTarget), cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+        int nct = 0;
+        for (const InjTarget &t : tg) nct = std::max(nct, t.start + t.count);
+        std::vector<InjContrib> ct(nct);
+        CK(cudaMemcpyAsync(ct.data(), g->d_ct[1], ct.size() * sizeof(InjContrib), cudaMemcpyDeviceToHost, g->stream));
+        CK(cudaStreamSynchronize(g->stream));
+        std::vector<int> ijk(3 * tg.size());
+        int box[6] = {INT32_MAX, -1, INT32_MAX, -1, INT32_MAX, -1};
+        for (size_t t = 0; t < tg.size(); ++t) {
+            const int64_t q = tg[t].idx;
+            const int k = (int)(q / d.pxy), j = (int)((q - k * d.pxy) / d.px), i = (int)(q - k * d.pxy - (int64_t)j * d.px);
+            const int v[3] = {i, j, k};
+            for (int a = 0; a < 3; ++a) {
+                ijk[3 * t + a] = v[a];
+                box[2 * a] = std::min(box[2 * a], v[a]);
+                box[2 * a + 1] = std::max(box[2 * a + 1], v[a]);
+            }
+        }
+        int base = 0;
+        for (int f = 0; f < 6; ++f) {
+            const int ax = f >> 1, ua = ax == 0 ? 1 : 0, va = ax == 2 ? 1 : 2;
+            g->hc_nu[f] = box[2 * ua + 1] - box[2 * ua] + 1;
+            g->hc_area[f] = g->hc_nu[f] * (box[2 * va + 1] - box[2 * va] + 1);
+            g->hc_base[f] = base;
+            base += 3 * g->hc_area[f];
+        }
+        std::vector<int32_t> slot(nct, -1);
+        bool ok = true;
+        for (size_t t = 0; t < tg.size() && ok; ++t)
+            for (int c = tg[t].start; c < tg[t].start + tg[t].count && ok; ++c) {
+                const int f = ct[c].face, ax = f >> 1, ua = ax == 0 ? 1 : 0, va = ax == 2 ? 1 : 2;
+                const int *v = &ijk[3 * t];
+                ok = f >= 0 && f < 6 && v[ax] == box[f] && tg[t].comp >= CPS_HX && tg[t].comp <= CPS_HZ;
+                if (ok)
+                    slot[c] = g->hc_base[f] + (tg[t].comp - CPS_HX) * g->hc_area[f] +
+                              (v[va] - box[2 * va]) * g->hc_nu[f] + (v[ua] - box[2 * ua]);
+            }
+        // a cell on two faces sums both, so each face takes its own contributions only once
+        for (int c = 0; c < nct && ok; ++c) ok = slot[c] >= 0;
+        if (ok) {
+            std::vector<int32_t> seen(base, 0);
+            for (int c = 0; c < nct && ok; ++c) ok = seen[slot[c]]++ == 0;
+        }
+        g->hc_ok = ok;
+        if (ok) {
+            for (int a = 0; a < 6; ++a) g->hc_box[a] = box[a];
+            g->hc_n = nct;
+            if ((s = dalloc(g, &g->d_hcorr, (size_t)base * g->esz))) return s;
+            CK(cudaMemsetAsync(g->d_hcorr, 0, (size_t)base * g->esz, g->stream));
+            if ((s = dalloc(g, (void **)&g->d_hslot, slot.size() * sizeof(int32_t)))) return s;
+            if ((s = upload_raw(g, g->d_hslot, slot.data(), slot.size() * sizeof(int32_t)))) return s;
+        }
+    }
+    const int by = g->shape.by;
+    if (g->om_by != by) {
+        if ((s = encode_step_maps(g, g->F, &g->om, by)) || (s = encode_step_maps(g, g->F2, &g->om2, by))) return s;
+        g->om_by = by;
+    }
+    g->onepass_ready = true;
+    return CPS_OK;
+}
+
+void swap_step_buffers(cps_grid *g)
+{
+    for (int c = 0; c < 6; ++c) std::swap(g->F[c], g->F2[c]);
+    if (g->pml_on)
+        for (int f = 0; f < 6; ++f) {
+            std::swap(g->d_q[f][2], g->d_q2[f][0]);
+            std::swap(g->d_q[f][3], g->d_q2[f][1]);
+        }
+    std::swap(g->om, g->om2);
+    g->tma_by = 0;  // the two-sweep maps were built over the other buffers
+}
+
+template <typename T>
+HCorr<T> h_corrections(const cps_grid *g)
+{
+    HCorr<T> q;
+    memset(&q, 0, sizeof(q));
+    if (g->tfsf_on && g->ntg[1] > 0) {
+        q.corr = (const T *)g->d_hcorr;
+        for (int a = 0; a < 6; ++a) {
+            q.box[a] = g->hc_box[a]; q.base[a] = g->hc_base[a]; q.nu[a] = g->hc_nu[a]; q.area[a] = g->hc_area[a];
+        }
+    }
+    return q;
+}
+
 cps_status check_device_error(cps_grid *g)
 {
     int e = 0;
@@ -388,9 +527,12 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
     cps_status s = ensure_sources(g);
     if (s) return s;
     // TMA boxes are 36 x (rows+1): grids narrower than that use the register sweeps
-    const bool use_tma = path == CPS_PATH_FUSED && g->sweep_mode == 0 && (g->shape.by == 4 || g->shape.by == 8) &&
+    const bool use_tma = path != CPS_PATH_PLAIN && g->sweep_mode == 0 && (g->shape.by == 4 || g->shape.by == 8) &&
                          g->d.px >= 64 && g->d.ny + 1 >= g->shape.by + 1;
-    if (use_tma && (s = ensure_tma(g))) return s;
+    bool onepass = use_tma && path == CPS_PATH_ONEPASS;
+    if (onepass && (s = ensure_onepass(g))) return s;
+    onepass = onepass && g->hc_ok;  // TF/SF targets off their box's surface: two sweeps instead
+    if (use_tma && !onepass && (s = ensure_tma(g))) return s;
     const FieldView<T> f = field_view<T>(g);
     const PmlView<T> p = pml_view<T>(g);
     const DlView<T> D = dl_view<T>(g);
@@ -412,6 +554,35 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             op_sources<T>(g, (int)n);
             if (g->pml_on) launch_e_pml<T>(f, p, g->stream);
             g->launches += 2 + (g->pml_on ? 12 : 0) + (g->dl_on ? 1 : 0) + (g->gain_on ? 3 : 0);
+        } else if (onepass) {
+            // one sweep into the other buffers, which become current; then the
+            // Drude-Lorentz cells (old E from the previous buffers), TF/SF E, sources
+            const bool timed = g->timing_stride > 0 && n % g->timing_stride == 0 &&
+                               g->ev_used + 4 <= (int)g->ev.size();
+            if (timed) cudaEventRecord(g->ev[g->ev_used], g->stream);
+            if (g->tfsf_on && g->ntg[1] > 0) {
+                launch_h_corrections<T>(g->d_ct[1], g->d_hslot, g->hc_n, (const T *)g->d_einc, g->tp.Nt, (double)n,
+                                        (T *)g->d_hcorr, g->stream);
+                g->launches++;
+            }
+            launch_step_tma<T>(g->om, field_view<T>(g), field_view_alt<T>(g), pml_view<T>(g), pml_view_alt<T>(g), D,
+                               G, h_corrections<T>(g), g->shape, g->d_err, g->stream);
+            g->launches++;
+            swap_step_buffers(g);
+            if (timed) {
+                cudaEventRecord(g->ev[g->ev_used + 1], g->stream);
+                cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
+            }
+            if (D.on && D.ncell > 0) {
+                launch_dl_cells_step<T>(field_view<T>(g), field_view_alt<T>(g), pml_view<T>(g), D, g->stream);
+                g->launches++;
+            }
+            if (timed) {
+                cudaEventRecord(g->ev[g->ev_used + 3], g->stream);
+                g->ev_used += 4;
+            }
+            op_inject<T>(g, 0, (double)n, CPS_FACE_ALL);
+            op_sources<T>(g, (int)n);
         } else {
             const bool timed = g->timing_stride > 0 && n % g->timing_stride == 0 &&
                                g->ev_used + 4 <= (int)g->ev.size();
@@ -1189,7 +1360,8 @@ extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
     if (s) return s;
     FLUSH_RECORDED(g);
     REQUIRE(nsteps >= 0, CPS_E_INVALID, "cps_step: negative step count");
-    REQUIRE(path == CPS_PATH_PLAIN || path == CPS_PATH_FUSED, CPS_E_INVALID, "cps_step: unknown path");
+    REQUIRE(path == CPS_PATH_PLAIN || path == CPS_PATH_FUSED || path == CPS_PATH_ONEPASS, CPS_E_INVALID,
+            "cps_step: unknown path");
     CK(cudaSetDevice(g->desc.device));
     return g->fp32 ? step_T<float>(g, nsteps, path) : step_T<double>(g, nsteps, path);
 }

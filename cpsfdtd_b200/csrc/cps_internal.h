@@ -182,6 +182,30 @@ void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, 
 template <typename T>
 void tma_attributes();
 
+// One-pass step (kernels_step.cu): H and E of a step in one sweep from the
+// buffers of fo (and pin's H-side psi) into those of fn (pout's H-side psi).
+// The H-side TF/SF corrections of the step come from dense per-face arrays
+// (launch_h_corrections fills them first); corr == nullptr: none.
+template <typename T>
+struct HCorr {
+    const T *corr;  // per face f: 3 components x nv x nu, from base[f]
+    int box[6];     // bounding box of the H targets: i0 i1 j0 j1 k0 k1
+    int base[6], nu[6], area[6];
+};
+template <typename T>
+void launch_step_tma(const StepMaps &M, const FieldView<T> &fo, const FieldView<T> &fn, const PmlView<T> &pin,
+                     const PmlView<T> &pout, const DlView<T> &D, const GainView<T> &G, const HCorr<T> &hc,
+                     FusedShape sh, int *err, cudaStream_t s);
+// the H-side TF/SF correction of every contribution at step n into its slot
+// of the per-face arrays (TF_SF::UpdateHField's terms, TF_SF.cpp:1201-1300)
+template <typename T>
+void launch_h_corrections(const InjContrib *ct, const int32_t *slot, int ncontrib, const T *table, int Nt, double n,
+                          T *corr, cudaStream_t s);
+// the Drude-Lorentz cells after a one-pass sweep (old E from fo, H and new E in fn)
+template <typename T>
+void launch_dl_cells_step(const FieldView<T> &fn, const FieldView<T> &fo, const PmlView<T> &p, const DlView<T> &D,
+                          cudaStream_t s);
+
 // Ports (kernels_ports.cu)
 constexpr int kMaxGather = 16;
 struct GatherDesc {

@@ -74,6 +74,7 @@ struct cps_grid {
     using InjContrib = cps::InjContrib;
     using FusedShape = cps::FusedShape;
     using TmaMaps = cps::TmaMaps;
+    using StepMaps = cps::StepMaps;
     template <typename T> using DlCoef = cps::DlCoef<T>;
     cps_grid_desc desc{};
     bool fp32 = false;
@@ -142,6 +143,20 @@ struct cps_grid {
     TmaMaps tma{};
     int tma_by = 0;
     int sweep_mode = 0;  // 0: TMA-fed sweeps, 1: register sweeps
+    // one-pass step (CPS_PATH_ONEPASS): a second field buffer and H-side psi
+    // set; a step reads F / d_q[f][2..3] and writes F2 / d_q2, then the two swap
+    void *F2[6] = {};
+    void *d_q2[6][2] = {};
+    StepMaps om{}, om2{};          // tensor maps over F and over F2
+    int om_by = 0;                 // tile rows the maps were built for
+    // H-side TF/SF corrections of the one-pass step: per-face arrays over the
+    // targets' bounding box and each contribution's slot in them
+    void *d_hcorr = nullptr;
+    int32_t *d_hslot = nullptr;
+    int hc_n = 0;                 // contributions
+    int hc_box[6] = {}, hc_base[6] = {}, hc_nu[6] = {}, hc_area[6] = {};
+    bool hc_ok = true;            // every target lies on the box's surface (else no one-pass)
+    bool onepass_ready = false;
     int *d_err = nullptr;  // set by a device wait that gave up
     // sweep timing samples: events (start, after H sweep, after E sweep)
     int timing_stride = 0;
@@ -163,6 +178,10 @@ void dfree(cps_grid *g, void *p);
 cps_status upload_raw(cps_grid *g, void *dst, const void *src, size_t bytes);
 cps_status ensure_sources(cps_grid *g);
 cps_status ensure_tma(cps_grid *g);
+// second buffer set, tensor maps and TF/SF target table of the one-pass step
+cps_status ensure_onepass(cps_grid *g);
+// make the buffers the last one-pass step wrote current
+void swap_step_buffers(cps_grid *g);
 cps_status flush_dft(cps_grid *g, PortState &P);
 cps_status check_device_error(cps_grid *g);
 // run the recorded calls of the grid (fused into one step when they form one)
@@ -205,6 +224,16 @@ inline FieldView<T> field_view(const cps_grid *g)
     return f;
 }
 
+// the second field buffer set of the one-pass step (written by the next step)
+template <typename T>
+inline FieldView<T> field_view_alt(const cps_grid *g)
+{
+    FieldView<T> f = field_view<T>(g);
+    f.Ex = (T *)g->F2[0]; f.Ey = (T *)g->F2[1]; f.Ez = (T *)g->F2[2];
+    f.Hx = (T *)g->F2[3]; f.Hy = (T *)g->F2[4]; f.Hz = (T *)g->F2[5];
+    return f;
+}
+
 template <typename T>
 inline PmlView<T> pml_view(const cps_grid *g)
 {
@@ -227,6 +256,29 @@ inline PmlView<T> pml_view(const cps_grid *g)
     p.cpmlE = (T)g->cpmlE;
     p.cpmlH = (T)g->cpmlH;
     return p;
+}
+
+// pml_view with the H-side psi of the second buffer set
+template <typename T>
+inline PmlView<T> pml_view_alt(const cps_grid *g)
+{
+    PmlView<T> p = pml_view<T>(g);
+    if (p.on)
+        for (int f = 0; f < 6; ++f) {
+            p.qh[f][0] = (T *)g->d_q2[f][0];
+            p.qh[f][1] = (T *)g->d_q2[f][1];
+        }
+    return p;
+}
+
+// words of one psi array of CPML face f: x slabs [k][j][s], y slabs [k][s][i], z slabs [s][j][i]
+inline size_t psi_words(const cps_grid *g, int f)
+{
+    const Dims &d = g->d;
+    const int np = g->pml.npml[f];
+    if (f < 2) return (size_t)(d.nz + 1) * (d.ny + 1) * psi_xw(np);
+    if (f < 4) return (size_t)(d.nz + 1) * (np + 1) * d.px;
+    return (size_t)(np + 1) * (d.ny + 1) * d.px;
 }
 
 template <typename T>

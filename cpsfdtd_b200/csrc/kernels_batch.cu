@@ -90,8 +90,8 @@ __global__ void __launch_bounds__(128) k_dl_batch(const BatchGrid<T> *__restrict
     const int64_t c = (int64_t)e.y + threadIdx.x;
     if (c >= e.z) return;
     const BatchGrid<T> &B = grids[e.x];
-    if (B.p.on) dl_cell_any<T, true>(B.f, B.p, B.D, c);
-    else dl_cell_any<T, false>(B.f, B.p, B.D, c);
+    if (B.p.on) dl_cell_any<T, true>(B.f, B.f, B.p, B.D, c);
+    else dl_cell_any<T, false>(B.f, B.f, B.p, B.D, c);
 }
 
 template <typename T>

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) k_dl_cells(FieldView<T> f, PmlView<T> p, 
 {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= D.ncell) return;
-    dl_cell_any<T, PML>(f, p, D, c);
+    dl_cell_any<T, PML>(f, f, p, D, c);
 }
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }

@@ -16,6 +16,16 @@ struct TmaMaps {
     CUtensorMap id;
 };
 
+// Tensor maps of the one-pass step sweep over one field buffer, x fastest:
+//   e[c]: Ex Ey Ez, box 40 x (BY+2) x 1 (from x0-4, y0-1)
+//   h[c]: Hx Hy Hz, box 36 x (BY+1) x 1 (from x0-4, y0-1)
+//   id:   uint8 IDs, box 48 x (BY+1) x 1 (from x0-16, y0-1)
+struct StepMaps {
+    CUtensorMap e[3];
+    CUtensorMap h[3];
+    CUtensorMap id;
+};
+
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
     return (uint32_t)__cvta_generic_to_shared(p);

@@ -283,11 +283,14 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
 }
 
 // Drude-Lorentz cell c of a grid's compacted list (Drude_Lorentz.cpp:153-227
-// in 3-D form, curl of the updated H), followed by its CPML correction.
+// in 3-D form, curl of the updated H), followed by its CPML correction.  The
+// cell's old E is read from fo (the same view as f in place; the other field
+// buffer after a one-pass step), H and the new E from/to f.
 // ND < 0: pole counts taken at run time from D.c (any count); ND >= 0: the
 // cell's ND Drude and NL Lorentz poles fixed at compile time, state loaded first.
 template <typename T, bool PML, int ND = -1, int NL = 0>
-__device__ __forceinline__ void dl_cell(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D, int64_t c)
+__device__ __forceinline__ void dl_cell(const FieldView<T> &f, const FieldView<T> &fo, const PmlView<T> &p,
+                                        const DlView<T> &D, int64_t c)
 {
     const Dims &d = f.d;
     const int64_t g = D.cell[c];
@@ -316,7 +319,7 @@ __device__ __forceinline__ void dl_cell(const FieldView<T> &f, const PmlView<T> 
     const T czz = C3 * dHy_i * cEzy - C3 * dHx_j * cEzx;
     const int64_t sc = D.ncell;
     T *st = D.state + c;
-    T ex = f.Ex[g], ey = f.Ey[g], ez = f.Ez[g];
+    T ex = fo.Ex[g], ey = fo.Ey[g], ez = fo.Ez[g];
     if (ND >= 0) {
         // every state word of the cell is requested before any is used
         constexpr int W = (ND < 0 ? 0 : ND) + 2 * NL + 1;
@@ -344,15 +347,16 @@ __device__ __forceinline__ void dl_cell(const FieldView<T> &f, const PmlView<T> 
 // dl_cell with the pole counts of the grid's material dispatched to a
 // compile-time form where one exists
 template <typename T, bool PML>
-__device__ __forceinline__ void dl_cell_any(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D, int64_t c)
+__device__ __forceinline__ void dl_cell_any(const FieldView<T> &f, const FieldView<T> &fo, const PmlView<T> &p,
+                                            const DlView<T> &D, int64_t c)
 {
     const int nd = D.c.nD, nl = D.c.nL;
-    if (nd == 1 && nl == 2) dl_cell<T, PML, 1, 2>(f, p, D, c);
-    else if (nd == 1 && nl == 1) dl_cell<T, PML, 1, 1>(f, p, D, c);
-    else if (nd == 1 && nl == 0) dl_cell<T, PML, 1, 0>(f, p, D, c);
-    else if (nd == 0 && nl == 1) dl_cell<T, PML, 0, 1>(f, p, D, c);
-    else if (nd == 0 && nl == 2) dl_cell<T, PML, 0, 2>(f, p, D, c);
-    else dl_cell<T, PML>(f, p, D, c);
+    if (nd == 1 && nl == 2) dl_cell<T, PML, 1, 2>(f, fo, p, D, c);
+    else if (nd == 1 && nl == 1) dl_cell<T, PML, 1, 1>(f, fo, p, D, c);
+    else if (nd == 1 && nl == 0) dl_cell<T, PML, 1, 0>(f, fo, p, D, c);
+    else if (nd == 0 && nl == 1) dl_cell<T, PML, 0, 1>(f, fo, p, D, c);
+    else if (nd == 0 && nl == 2) dl_cell<T, PML, 0, 2>(f, fo, p, D, c);
+    else dl_cell<T, PML>(f, fo, p, D, c);
 }
 
 }  // namespace cps

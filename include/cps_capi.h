@@ -80,9 +80,12 @@ enum {
 enum { CPS_FP64 = 0, CPS_FP32 = 1 };
 enum { CPS_EX = 0, CPS_EY = 1, CPS_EZ = 2, CPS_HX = 3, CPS_HY = 4, CPS_HZ = 5 };
 /* cps_step paths: PLAIN launches one kernel per reference routine in the
- * reference order; FUSED runs the fused sweeps (same results within the
- * precision's tolerance). */
-enum { CPS_PATH_PLAIN = 0, CPS_PATH_FUSED = 1 };
+ * reference order; FUSED runs the fused sweeps, one for H and one for E
+ * (same results within the precision's tolerance); ONEPASS runs H and E of
+ * a step in one sweep into a second set of field buffers that then becomes
+ * current (twice the field memory, about two thirds of FUSED's field traffic;
+ * grids the TMA sweeps cannot tile, and sweep mode 1, run FUSED instead). */
+enum { CPS_PATH_PLAIN = 0, CPS_PATH_FUSED = 1, CPS_PATH_ONEPASS = 2 };
 /* TF/SF face bits for cps_op_tfsf_* (TF_SF.h:41-52 face variants) */
 enum { CPS_FACE_X1 = 1, CPS_FACE_X2 = 2, CPS_FACE_Y1 = 4, CPS_FACE_Y2 = 8,
        CPS_FACE_Z1 = 16, CPS_FACE_Z2 = 32, CPS_FACE_ALL = 63 };

@@ -57,23 +57,27 @@ def _check(g, dk, pts, o, tol, tag):
             assert err <= tol, f"{tag} port {n} DFT rel L2 {err:.3e}"
 
 
+PATHS = {0: "plain", 1: "fused", 2: "onepass"}
+
+
 @pytest.mark.parametrize("case", sorted(CASES))
-@pytest.mark.parametrize("path", [0, 1], ids=["plain", "fused"])
+@pytest.mark.parametrize("path", [0, 1, 2], ids=["plain", "fused", "onepass"])
 def test_fp64_matches_oracle(case, path, oracle_runs):
     import cpsfdtd_b200 as cps
     dk, ids, pts, o = oracle_runs[case]
     g = cps.Grid.from_deck(dk, cps.FP64, ids=ids, port_points_list=pts)
     g.step(dk.nsteps, path)
-    _check(g, dk, pts, o, FP64_TOL, f"{case}/fp64/{'plain' if path == 0 else 'fused'}")
+    _check(g, dk, pts, o, FP64_TOL, f"{case}/fp64/{PATHS[path]}")
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_fp32_fused_matches_oracle(case, oracle_runs):
+@pytest.mark.parametrize("path", [1, 2], ids=["fused", "onepass"])
+def test_fp32_matches_oracle(case, path, oracle_runs):
     import cpsfdtd_b200 as cps
     dk, ids, pts, o = oracle_runs[case]
     g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts)
-    g.step(dk.nsteps, cps.FUSED)
-    _check(g, dk, pts, o, FP32_TOL, f"{case}/fp32/fused")
+    g.step(dk.nsteps, path)
+    _check(g, dk, pts, o, FP32_TOL, f"{case}/fp32/{PATHS[path]}")
 
 
 def test_fp64_plain_is_bit_exact_on_dielectric_cpml(oracle_runs):
@@ -91,9 +95,10 @@ def test_gain_populations_match_oracle(oracle_mod, oracle_runs):
     import cpsfdtd_b200 as cps
     dk, ids, pts, o = oracle_runs["c3"]
     want = o.populations()
-    for prec, tol in ((cps.FP64, 1e-12), (cps.FP32, 1e-6)):
+    for prec, tol, path in ((cps.FP64, 1e-12, cps.FUSED), (cps.FP32, 1e-6, cps.FUSED),
+                            (cps.FP64, 1e-12, cps.ONEPASS), (cps.FP32, 1e-6, cps.ONEPASS)):
         g = cps.Grid.from_deck(dk, prec, ids=ids, port_points_list=pts)
-        g.step(dk.nsteps, cps.FUSED)
+        g.step(dk.nsteps, path)
         got = g.populations()
         assert got.shape == want.shape
         assert np.abs(got - want).max() <= tol
