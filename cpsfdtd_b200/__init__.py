@@ -354,11 +354,18 @@ class Grid:
         _check(self.L.cps_port_read(self.h, pid, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
-    def port_dft(self, pid, raw=False):
+    def port_dft(self, pid, raw=False, out=None):
         """DFT accumulators; raw=True gives the ABI layout [ncomp][nfreq][2][npts],
-        otherwise a [npts][ncomp][nfreq][2] view of it."""
+        otherwise a [npts][ncomp][nfreq][2] view of it.  out: a C-contiguous
+        float64 array of that many values to read into (pinned host memory
+        makes the copy a direct DMA)."""
         npts, ncomp, nfreq = self.ports[pid]
-        out = np.empty((ncomp, nfreq, 2, npts))
+        shape = (ncomp, nfreq, 2, npts)
+        if out is None:
+            out = np.empty(shape)
+        else:
+            assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == np.prod(shape)
+            out = out.reshape(shape)
         _check(self.L.cps_port_dft_read(self.h, pid, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out if raw else out.transpose(3, 0, 1, 2)
 

@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "grid.h"
@@ -24,6 +25,25 @@ void set_error(const std::string &msg) { g_last_error = msg; }
 }  // namespace cps
 
 using namespace cps;
+
+namespace {
+// f(begin, end) over [0, n) split across up to 16 host threads (the calling one included)
+template <typename F>
+void parallel_for(int n, F f)
+{
+    const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
+    const int parts = std::min(nt, n);
+    if (parts <= 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 1; t < parts; ++t)
+        th.emplace_back([&f, n, t, parts] { f((int)((int64_t)n * t / parts), (int)((int64_t)n * (t + 1) / parts)); });
+    f(0, (int)((int64_t)n / parts));
+    for (std::thread &x : th) x.join();
+}
+}  // namespace
 
 // calls recorded on the grid run before anything that reads or changes its state
 #define FLUSH_RECORDED(g)                                  \
@@ -156,27 +176,48 @@ cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cel
                       uint2 **d_segm = nullptr)
 {
     const Dims &d = g->d;
-    std::vector<int64_t> cells;
     const int nseg = d.px / 32;
     std::vector<int32_t> seg((size_t)(d.nz + 1) * (d.ny + 1) * nseg, 0);
     std::vector<uint2> segm(d_segm ? seg.size() : 0);
-    for (int k = 0; k <= d.nz; ++k)
-        for (int j = 0; j <= d.ny; ++j)
-            for (int s = 0; s < nseg; ++s) {
-                const size_t w = ((size_t)k * (d.ny + 1) + j) * nseg + s;
-                seg[w] = (int32_t)cells.size();
-                uint32_t bits = 0;
-                if (k >= 1 && k < d.nz && j >= 1 && j < d.ny)
-                    for (int i = s * 32; i < s * 32 + 32 && i < d.nx; ++i) {
-                        if (i < 1) continue;
-                        const int64_t q = d.idx(i, j, k);
-                        if (g->ids_dev[q] == id_match) {
-                            cells.push_back(q);
-                            bits |= 1u << (i - s * 32);
+    // planes split across threads: each lists its cells with plane-local offsets,
+    // then the parts are joined in plane order and the offsets rebased
+    const int nz1 = d.nz + 1;
+    std::vector<std::vector<int64_t>> part(nz1);
+    parallel_for(nz1, [&](int k0, int k1) {
+        for (int k = k0; k < k1; ++k) {
+            std::vector<int64_t> &cells = part[k];
+            for (int j = 0; j <= d.ny; ++j)
+                for (int s = 0; s < nseg; ++s) {
+                    const size_t w = ((size_t)k * (d.ny + 1) + j) * nseg + s;
+                    seg[w] = (int32_t)cells.size();
+                    uint32_t bits = 0;
+                    if (k >= 1 && k < d.nz && j >= 1 && j < d.ny)
+                        for (int i = s * 32; i < s * 32 + 32 && i < d.nx; ++i) {
+                            if (i < 1) continue;
+                            const int64_t q = d.idx(i, j, k);
+                            if (g->ids_dev[q] == id_match) {
+                                cells.push_back(q);
+                                bits |= 1u << (i - s * 32);
+                            }
                         }
-                    }
-                if (d_segm) segm[w] = make_uint2((unsigned)seg[w], bits);
+                    if (d_segm) segm[w] = make_uint2(0u, bits);
+                }
+        }
+    });
+    std::vector<int64_t> base(nz1 + 1, 0);
+    for (int k = 0; k < nz1; ++k) base[k + 1] = base[k] + (int64_t)part[k].size();
+    REQUIRE(base[nz1] < (int64_t)INT32_MAX, CPS_E_INVALID, "too many cells in one compacted list");
+    std::vector<int64_t> cells((size_t)base[nz1]);
+    parallel_for(nz1, [&](int k0, int k1) {
+        for (int k = k0; k < k1; ++k) {
+            std::copy(part[k].begin(), part[k].end(), cells.begin() + base[k]);
+            const size_t w0 = (size_t)k * (d.ny + 1) * nseg, w1 = w0 + (size_t)(d.ny + 1) * nseg;
+            for (size_t w = w0; w < w1; ++w) {
+                seg[w] += (int32_t)base[k];
+                if (d_segm) segm[w].x = (unsigned)seg[w];
             }
+        }
+    });
     REQUIRE(cells.size() < (size_t)INT32_MAX, CPS_E_INVALID, "too many cells in one compacted list");
     *count = (int64_t)cells.size();
     cps_status s = dalloc(g, (void **)d_cell, cells.size() * sizeof(int64_t));
@@ -798,15 +839,28 @@ extern "C" cps_status cps_grid_upload_ids(cps_grid *g, const uint8_t *ids)
             "cps_grid_upload_ids: IDs must be set before the physics modules are initialised");
     const Dims &d = g->d;
     std::fill(g->ids_dev.begin(), g->ids_dev.end(), 0);
+    // [i][j][k] to the device layout in 64 x 64 (i, k) blocks per row j, rows split across threads
+    std::mutex mu;
     int maxid = 0;
-    size_t q = 0;
-    for (int i = 0; i <= d.nx; ++i)
-        for (int j = 0; j <= d.ny; ++j)
-            for (int k = 0; k <= d.nz; ++k) {
-                const uint8_t v = ids[q++];
-                maxid = std::max<int>(maxid, v);
-                g->ids_dev[d.idx(i, j, k)] = v;
-            }
+    uint8_t *dst = g->ids_dev.data();
+    parallel_for(d.ny + 1, [&](int j0, int j1) {
+        int mx = 0;
+        for (int j = j0; j < j1; ++j)
+            for (int ib = 0; ib <= d.nx; ib += 64)
+                for (int kb = 0; kb <= d.nz; kb += 64) {
+                    const int ie = std::min(ib + 64, d.nx + 1), kend = std::min(kb + 64, d.nz + 1);
+                    for (int i = ib; i < ie; ++i) {
+                        const uint8_t *src = ids + ((size_t)i * (d.ny + 1) + j) * (d.nz + 1);
+                        for (int k = kb; k < kend; ++k) {
+                            const uint8_t v = src[k];
+                            mx = std::max<int>(mx, v);
+                            dst[d.idx(i, j, k)] = v;
+                        }
+                    }
+                }
+        std::lock_guard<std::mutex> lk(mu);
+        maxid = std::max(maxid, mx);
+    });
     REQUIRE(g->nmedia == 0 || maxid < g->nmedia, CPS_E_INVALID,
             "cps_grid_upload_ids: an ID has no medium (set the media first or extend them)");
     cps_status s = upload_raw(g, g->d_id, g->ids_dev.data(), g->ids_dev.size());
@@ -1072,54 +1126,77 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
         InjContrib c;
     };
     for (int isH = 0; isH < 2; ++isH) {
-        std::vector<Item> items;  // in the reference's face order
-        for (int oi = 0; oi < 6; ++oi) {
-            const int f = order[oi], ax = f / 2, far = f & 1;
-            int u1, u2, v1, v2;
-            if (ax == 0) { u1 = j1; u2 = j2; v1 = k1; v2 = k2; }
-            else if (ax == 1) { u1 = i1; u2 = i2; v1 = k1; v2 = k2; }
-            else { u1 = i1; u2 = i2; v1 = j1; v2 = j2; }
-            for (int which = 0; which < 2; ++which) {
-                // E1 covers [u1,u2) x [v1,v2], E2 [u1,u2] x [v1,v2); the x-face H
-                // strips add nothing in the reference (TF_SF.cpp:1244-1251,
-                // 1260-1267 read unset point members), so x-face H covers [u1,u2) x [v1,v2)
-                int ue = which == 0 ? u2 - 1 : u2, ve = which == 0 ? v2 : v2 - 1;
-                if (isH && ax == 0) { ue = u2 - 1; ve = v2 - 1; }
-                const int comp = isH ? compH[ax][which] : compE[ax][which];
-                const double coef = isH ? cH[f][which] : cE[f][which];
-                for (int u = u1; u <= ue; ++u)
-                    for (int v = v1; v <= ve; ++v) {
-                        int i, j, k;
-                        double x, y, z;
-                        if (ax == 0) {
-                            i = far ? i2 : i1; j = u; k = v;
-                            x = isH ? dx * (i - p->i0) : dx * (far ? (i - p->i0 + 0.5) : (i - p->i0 - 0.5));
-                            y = dy * (j - p->j0); z = dz * (k - p->k0);
-                            if (isH) i += far ? 1 : -1;
-                        } else if (ax == 1) {
-                            i = u; j = far ? j2 : j1; k = v;
-                            x = dx * (i - p->i0);
-                            y = isH ? dy * (j - p->j0) : dy * (far ? (j - p->j0 + 0.5) : (j - p->j0 - 0.5));
-                            z = dz * (k - p->k0);
-                            if (isH) j += far ? 1 : -1;
-                        } else {
-                            i = u; j = v; k = far ? k2 : k1;
-                            x = dx * (i - p->i0); y = dy * (j - p->j0);
-                            z = isH ? dz * (k - p->k0) : dz * (far ? (k - p->k0 + 0.5) : (k - p->k0 - 0.5));
-                            if (isH) k += far ? 1 : -1;
+        // the twelve (face, component) strips are generated in parallel and
+        // joined in the reference's face order
+        std::vector<std::vector<Item>> strips(12);
+        parallel_for(12, [&](int t0, int t1) {
+            for (int t = t0; t < t1; ++t) {
+                const int oi = t / 2, which = t % 2;
+                std::vector<Item> &items = strips[t];
+                const int f = order[oi], ax = f / 2, far = f & 1;
+                int u1, u2, v1, v2;
+                if (ax == 0) { u1 = j1; u2 = j2; v1 = k1; v2 = k2; }
+                else if (ax == 1) { u1 = i1; u2 = i2; v1 = k1; v2 = k2; }
+                else { u1 = i1; u2 = i2; v1 = j1; v2 = j2; }
+                {
+                    // E1 covers [u1,u2) x [v1,v2], E2 [u1,u2] x [v1,v2); the x-face H
+                    // strips add nothing in the reference (TF_SF.cpp:1244-1251,
+                    // 1260-1267 read unset point members), so x-face H covers [u1,u2) x [v1,v2)
+                    int ue = which == 0 ? u2 - 1 : u2, ve = which == 0 ? v2 : v2 - 1;
+                    if (isH && ax == 0) { ue = u2 - 1; ve = v2 - 1; }
+                    const int comp = isH ? compH[ax][which] : compE[ax][which];
+                    const double coef = isH ? cH[f][which] : cE[f][which];
+                    for (int u = u1; u <= ue; ++u)
+                        for (int v = v1; v <= ve; ++v) {
+                            int i, j, k;
+                            double x, y, z;
+                            if (ax == 0) {
+                                i = far ? i2 : i1; j = u; k = v;
+                                x = isH ? dx * (i - p->i0) : dx * (far ? (i - p->i0 + 0.5) : (i - p->i0 - 0.5));
+                                y = dy * (j - p->j0); z = dz * (k - p->k0);
+                                if (isH) i += far ? 1 : -1;
+                            } else if (ax == 1) {
+                                i = u; j = far ? j2 : j1; k = v;
+                                x = dx * (i - p->i0);
+                                y = isH ? dy * (j - p->j0) : dy * (far ? (j - p->j0 + 0.5) : (j - p->j0 - 0.5));
+                                z = dz * (k - p->k0);
+                                if (isH) j += far ? 1 : -1;
+                            } else {
+                                i = u; j = v; k = far ? k2 : k1;
+                                x = dx * (i - p->i0); y = dy * (j - p->j0);
+                                z = isH ? dz * (k - p->k0) : dz * (far ? (k - p->k0 + 0.5) : (k - p->k0 - 0.5));
+                                if (isH) k += far ? 1 : -1;
+                            }
+                            InjContrib c;
+                            tfsf_point(x, y, z, kx, ky, kz, kabs, p->w0, p->z0, zR, l0, dt, &c.delay, &c.profile);
+                            c.coef = coef;
+                            c.face = f;
+                            c.pad = 0;
+                            items.push_back({d.idx(i, j, k) * 8 + comp, c});
                         }
-                        InjContrib c;
-                        tfsf_point(x, y, z, kx, ky, kz, kabs, p->w0, p->z0, zR, l0, dt, &c.delay, &c.profile);
-                        c.coef = coef;
-                        c.face = f;
-                        c.pad = 0;
-                        items.push_back({d.idx(i, j, k) * 8 + comp, c});
-                    }
+                }
             }
-        }
+        });
         // targets in device order, so neighbouring threads touch neighbouring cells;
-        // the stable sort keeps each target's contributions in the reference's face order
-        std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.key < b.key; });
+        // a stable sort by key keeps each target's contributions in the reference's
+        // face order: a counting sort by plane, then a stable sort within each plane
+        const int nz1 = d.nz + 1;
+        std::vector<size_t> start(nz1 + 1, 0);
+        for (const std::vector<Item> &st : strips)
+            for (const Item &it : st) start[(size_t)(it.key / 8 / d.pxy) + 1]++;
+        for (int k = 0; k < nz1; ++k) start[k + 1] += start[k];
+        std::vector<Item> items(start[nz1]);
+        {
+            std::vector<size_t> at(start.begin(), start.end() - 1);
+            for (const std::vector<Item> &st : strips)
+                for (const Item &it : st) items[at[(size_t)(it.key / 8 / d.pxy)]++] = it;
+        }
+        strips.clear();
+        parallel_for(nz1, [&](int k0, int k1) {
+            for (int k = k0; k < k1; ++k)
+                std::stable_sort(items.begin() + start[k], items.begin() + start[k + 1],
+                                 [](const Item &a, const Item &b) { return a.key < b.key; });
+        });
         std::vector<InjTarget> tg;
         std::vector<InjContrib> ct;
         ct.reserve(items.size());
