@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--workload", default="dispersive", choices=["dispersive", "laser"],
                     help="bench deck: dispersive scattering (default) or the photonic-crystal laser")
     ap.add_argument("--job-steps", type=int, default=4000)
+    ap.add_argument("--path", default="fused", choices=["fused", "onepass"],
+                    help="one-grid stepping path: two TMA sweeps per step (default) or the one-pass step")
     ap.add_argument("--e2e-steps", type=int, default=2, help="end-to-end jobs to time")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-steps", type=int, default=3, help="time steps in the CPU baseline sample")
@@ -139,9 +141,9 @@ def workload_name(dk, kind):
             f"Gaussian beam, 6 ports x 64-freq FP64 DFT; 1 bench step = 1 job of {dk.nsteps} time steps")
 
 
-def config_of(dk, kind, world):
+def config_of(dk, kind, world, path="fused"):
     return {"workload": workload_name(dk, kind), "grid": [dk.nx, dk.ny, dk.nz], "time_steps_per_job": dk.nsteps,
-            "precision": "fp32 fields, fp64 port accumulators", "path": "fused",
+            "precision": "fp32 fields, fp64 port accumulators", "path": path,
             "l2": f"inputs larger than L2 (fields {6 * 4 * (dk.nx + 1) * (dk.ny + 1) * (dk.nz + 1) / 1e9:.2f} GB "
                   "per grid)", "parallelism": f"replicas x{world}"}
 
@@ -177,6 +179,15 @@ def sweep_bytes(dk, ndl, prec_bytes=4, ngain=0):
     stride = len(dk.dl["fD"]) + 2 * len(dk.dl["fL"]) + 1 if dk.dl else 0
     e = e_cells * (9 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s + ngain * 15 * 2 * s
     return h, e
+
+
+def onepass_bytes(dk, ngain, prec_bytes=4):
+    """Algorithmic bytes of one one-pass sweep (FP32): the six fields read and
+    written once, 1 B ID, CPML psi of both sides (2 words read + write per slab
+    cell and side), gain state; the Drude-Lorentz cells run in their own kernel."""
+    h, e = sweep_bytes(dk, 0, prec_bytes, ngain)
+    nx, ny, nz, s = dk.nx, dk.ny, dk.nz, prec_bytes
+    return h + e - nx * ny * nz * (9 * s + 1) - (nx - 1) * (ny - 1) * (nz - 1) * (9 * s + 1) + nx * ny * nz * (12 * s + 1)
 
 
 def dist_setup():
@@ -255,7 +266,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded deck generator)",
-            "config": config_of(dk, args.workload, args.gpus),
+            "config": config_of(dk, args.workload, args.gpus, args.path),
             "cpu_baseline": {"value": v, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -453,9 +464,11 @@ def run_ours(args):
     g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts, device=local)
     stream = torch.cuda.ExternalStream(g.stream(), device=local)
 
+    path = cps.ONEPASS if args.path == "onepass" else cps.FUSED
+
     def job(grid):
         grid.reset(dk.n0)
-        grid.step(dk.nsteps, cps.FUSED)
+        grid.step(dk.nsteps, path)
         grid.flush_ports()
 
     for _ in range(args.warmup):
@@ -494,7 +507,10 @@ def run_ours(args):
     ndl = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_DISPERSIVE).sum()) if dk.dl else 0
     ngain = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_GAIN).sum()) if dk.gain else 0
     hb, eb = sweep_bytes(dk, ndl, ngain=ngain)
-    dom_ms, dom_bytes, dom = (e_ms, eb, "E sweep") if e_ms >= h_ms else (h_ms, hb, "H sweep")
+    if path == cps.ONEPASS:  # h_ms: the one-pass sweep (with its TF/SF terms); e_ms: the Drude-Lorentz cells
+        dom_ms, dom_bytes, dom = h_ms, onepass_bytes(dk, ngain), "one-pass sweep"
+    else:
+        dom_ms, dom_bytes, dom = (e_ms, eb, "E sweep") if e_ms >= h_ms else (h_ms, hb, "H sweep")
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",
             "frac": achieved / P["hbm_gbs"], "peak_source": src, "traffic": None,
@@ -503,7 +519,7 @@ def run_ours(args):
             "step_bytes_per_cell": (hb + eb) / cells,
             "step_frac_at_50B": value / world * 50 / P["hbm_gbs"]}
     tr = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr) and args.workload == "dispersive" and args.n == 256:
+    if os.path.exists(tr) and args.workload == "dispersive" and args.n == 256 and path == cps.FUSED:
         try:
             roof["traffic"] = json.load(open(tr)).get("e_sweep_bytes_per_launch")
         except (ValueError, OSError):
@@ -523,7 +539,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             gg = cps.Grid.from_deck(dk, cps.FP32, ids=pinned_ids.numpy(), port_points_list=pts, device=local)
-            gg.step(dk.nsteps, cps.FUSED)
+            gg.step(dk.nsteps, path)
             outs = [gg.port_dft(n, raw=True, out=pinned_out[n]) for n in range(len(dk.ports))
                     if pinned_out[n] is not None]
             gg.close()
@@ -562,7 +578,7 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
                 "data": "synthetic (seeded deck generator)",
-                "config": config_of(dk, args.workload, world),
+                "config": config_of(dk, args.workload, world, args.path),
                 "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
                 "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens, "serving": srv}
         print(json.dumps(line), flush=True)

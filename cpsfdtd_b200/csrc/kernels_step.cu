@@ -92,7 +92,7 @@ template <typename T, int BY, bool PML, bool TFSF, bool STORE>
 __device__ __forceinline__ void h_cell(const FieldView<T> &f, const PmlView<T> &pout, const HSum<T> &hs,
                                        const unsigned char *b, const unsigned char *bn, int lx, int ly, int i, int j,
                                        int k, const HCol<T> &hc, const ColPml<T> &pc, const PsiRegs<T> &r, T &hx,
-                                       T &hy, T &hz)
+                                       T &hy, T &hz, bool store = true)
 {
     using L = StepLayout<T, BY>;
     const Dims &d = f.d;
@@ -112,7 +112,8 @@ __device__ __forceinline__ void h_cell(const FieldView<T> &f, const PmlView<T> &
     hx = aH * hxt[hr] - bH * dEz_j * hc.cHxz + bH * dEy_k * sv.cHxy[k];
     hy = aH * hyt[hr] - bH * dEx_k * sv.cHyx[k] + bH * dEz_i * hc.cHyz;
     hz = aH * hzt[hr] + bH * dEx_j * hc.cHzx - bH * dEy_i * hc.cHzy;
-    if (PML) pml_h_cell_pre<T, STORE>(pout, d, pc, i, j, k, r, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz);
+    if (PML)
+        pml_h_cell_pre<T, STORE>(pout, d, pc, i, j, k, r, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz, store);
     if (TFSF) {
         hx = hx + hs.x;
         hy = hy + hs.y;
@@ -248,10 +249,8 @@ __device__ __forceinline__ void step_body(const StepMaps &M, const FieldView<T> 
         const unsigned char *b = sm + (q % kStages) * L::STAGE_B, *bn = sm + ((q + 1) % kStages) * L::STAGE_B;
         T *hn = (T *)(hn_base + (k & 1) * L::HN_B);
         T hx = T(0), hy = T(0), hz = T(0);
-        if (act_h) {
-            if (store) h_cell<T, BY, PML, TFSF, true>(fo, pout, hs, b, bn, tx, ty, i, j, k, hco, pch, qho, hx, hy, hz);
-            else h_cell<T, BY, PML, TFSF, false>(fo, pout, hs, b, bn, tx, ty, i, j, k, hco, pch, qho, hx, hy, hz);
-        }
+        if (act_h)  // psi is written from the chunk's own planes only
+            h_cell<T, BY, PML, TFSF, true>(fo, pout, hs, b, bn, tx, ty, i, j, k, hco, pch, qho, hx, hy, hz, store);
         const int64_t g = d.idx(i, j, k);
         if (store) {
             if (act_h) {

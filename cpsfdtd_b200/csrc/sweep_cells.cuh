@@ -217,20 +217,20 @@ __device__ __forceinline__ void pml_e_cell_pre(const PmlView<T> &p, const Dims &
 template <typename T, bool STORE = true>
 __device__ __forceinline__ void pml_h_cell_pre(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, int i, int j,
                                                int k, const PsiRegs<T> &r, T dEz_i, T dEy_i, T dEx_j, T dEz_j,
-                                               T dEy_k, T dEx_k, T &hx, T &hy, T &hz)
+                                               T dEy_k, T dEx_k, T &hx, T &hy, T &hz, bool store = true)
 {
     const T ch = p.cpmlH;
     if (c.fx >= 0) {
         const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(p.np[c.fx]) + c.sxl;
         const T a0 = c.bx * r.x0 + c.cx * dEz_i, a1 = c.bx * r.x1 + c.cx * dEy_i;
-        if (STORE) { p.qh[c.fx][0][q] = a0; p.qh[c.fx][1][q] = a1; }
+        if (STORE && store) { p.qh[c.fx][0][q] = a0; p.qh[c.fx][1][q] = a1; }
         hy = hy + a0 * ch;
         hz = hz - a1 * ch;
     }
     if (c.fy >= 0) {
         const int64_t q = ((int64_t)k * (p.np[c.fy] + 1) + c.syl) * d.px + i;
         const T a0 = c.by * r.y0 + c.cy * dEx_j, a1 = c.by * r.y1 + c.cy * dEz_j;
-        if (STORE) { p.qh[c.fy][0][q] = a0; p.qh[c.fy][1][q] = a1; }
+        if (STORE && store) { p.qh[c.fy][0][q] = a0; p.qh[c.fy][1][q] = a1; }
         hz = hz - a0 * ch;
         hx = hx + a1 * ch;
     }
@@ -241,7 +241,7 @@ __device__ __forceinline__ void pml_h_cell_pre(const PmlView<T> &p, const Dims &
         const int64_t q = ((int64_t)szl * (d.ny + 1) + j) * d.px + i;
         const T b = p.bH[fz][szl], cc = p.cH[fz][szl];
         const T a0 = b * r.z0 + cc * dEy_k, a1 = b * r.z1 + cc * dEx_k;
-        if (STORE) { p.qh[fz][0][q] = a0; p.qh[fz][1][q] = a1; }
+        if (STORE && store) { p.qh[fz][0][q] = a0; p.qh[fz][1][q] = a1; }
         hx = hx - a0 * ch;
         hy = hy + a1 * ch;
     }
