@@ -56,6 +56,10 @@ class DlParams(C.Structure):
                 ("literal", C.c_int32)]
 
 
+class DrudeParams(C.Structure):
+    _fields_ = [("epsInf", C.c_double), ("omegaP_hz", C.c_double), ("sigma", C.c_double), ("gamma_hz", C.c_double)]
+
+
 class GainParams(C.Structure):
     _fields_ = [("gain_id", C.c_int32), ("lambda_a", C.c_double), ("lambda_b", C.c_double),
                 ("gamma_a", C.c_double), ("gamma_b", C.c_double), ("t30", C.c_double), ("t32", C.c_double),
@@ -100,6 +104,7 @@ def lib():
             "cps_mesh_rasterize": ([I32, I32, I32, D, D, D, I32, C.POINTER(Shape), P, I32], I32),
             "cps_pml_init": ([P, C.POINTER(PmlParams)], I32),
             "cps_dl_init": ([P, C.POINTER(DlParams)], I32),
+            "cps_drude_init": ([P, C.POINTER(DrudeParams)], I32),
             "cps_gain_init": ([P, C.POINTER(GainParams)], I32),
             "cps_tfsf_init": ([P, C.POINTER(TfsfParams)], I32),
             "cps_tfsf_set_tables": ([P, I32, dp, dp], I32), "cps_tfsf_get_tables": ([P, I32, dp, dp], I32),
@@ -268,6 +273,11 @@ class Grid:
         pp = DlParams(d["sigma"], d["epsInf"], len(d["fD"]), len(d["fL"]), arr(d["fD"]), arr(d["gD"]),
                       arr(d["fL"]), arr(d["dL"]), arr(d["depsL"]), int(d.get("literal", 0)))
         _check(self.L.cps_dl_init(self.h, C.byref(pp)))
+
+    def drude_init(self, d):
+        """The single-pole Drude class (Drude.cpp): dict epsInf fP sigma gamma (Hz)."""
+        pp = DrudeParams(d["epsInf"], d["fP"], d["sigma"], d["gamma"])
+        _check(self.L.cps_drude_init(self.h, C.byref(pp)))
 
     def gain_init(self, g):
         pp = GainParams(int(g.get("gain_id", 5)), g["lambda_a"], g["lambda_b"], g["gamma_a"], g["gamma_b"],

@@ -964,6 +964,9 @@ extern "C" cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p)
     REQUIRE(p->nD >= 0 && p->nL >= 0 && p->nD <= kMaxPoles && p->nL <= kMaxPoles && p->nD + p->nL > 0,
             CPS_E_INVALID, "cps_dl_init: 0..8 Drude and 0..8 Lorentz poles, at least one");
     REQUIRE(p->epsInf > 0, CPS_E_INVALID, "cps_dl_init: epsInf must be positive");
+    REQUIRE(p->literal >= 0 && p->literal <= 2, CPS_E_INVALID, "cps_dl_init: literal must be 0, 1 or 2");
+    REQUIRE(p->literal != 2 || (p->nD == 1 && p->nL == 0), CPS_E_INVALID,
+            "cps_dl_init: the single-pole Drude form (literal 2) takes one Drude pole and no Lorentz pole");
     const double dt = g->desc.dt;
     DlCoef<double> &D = g->dlc;
     memset(&D, 0, sizeof(D));
@@ -983,23 +986,46 @@ extern "C" cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p)
         D.gammaL[q] = (kEps0 * p->depsL[q] * omega * omega * dt * dt) / (1.0 + delta * dt);
         temp2 = temp2 + D.gammaL[q];
     }
+    if (p->literal == 2) {
+        // the single-pole Drude class: Drude.cpp:56-60 in its own order; its
+        // C1Drude, C2Drude, C3Drude are this recursion's C1, C3 and C4[0]
+        const double b = D.beta[0], kp = D.kappa[0], e = p->epsInf, sg = p->sigma;
+        D.C1 = (2 * kEps0 * e - dt * b - sg * dt) / (2 * kEps0 * e + dt * b + sg * dt);
+        D.C2 = 0.0;
+        D.C3 = (2 * dt) / (2 * kEps0 * e + dt * b + sg * dt);
+        D.C4[0] = ((1 + kp) * dt) / (2 * kEps0 * e + dt * b + sg * dt);
+    }
     const double den = 2.0 * kEps0 * p->epsInf + p->sigma * dt + dt * temp1 + temp2 / 2.0;
     // literal: C1 and C5 as Drude_Lorentz.cpp:96,106; else the values of the
     // ADE discretisation (E^n coefficient with -sigma dt - dt sum(beta), J_L
     // coefficient with the factor dt)
-    if (p->literal) D.C1 = (2.0 * kEps0 * p->epsInf + p->sigma * dt + dt * temp1) / den;
-    else D.C1 = (2.0 * kEps0 * p->epsInf - p->sigma * dt - dt * temp1) / den;
-    D.C2 = temp2 / 2.0 / den;
-    D.C3 = 2.0 * dt / den;
-    for (int q = 0; q < p->nD; ++q) D.C4[q] = (1.0 + D.kappa[q]) * dt / den;
-    for (int q = 0; q < p->nL; ++q) {
-        D.C5[q] = p->literal ? (1.0 + D.alpha[q]) / den : (1.0 + D.alpha[q]) * dt / den;
-        D.C6[q] = D.xi[q] * dt / den;
+    if (p->literal != 2) {
+        if (p->literal) D.C1 = (2.0 * kEps0 * p->epsInf + p->sigma * dt + dt * temp1) / den;
+        else D.C1 = (2.0 * kEps0 * p->epsInf - p->sigma * dt - dt * temp1) / den;
+        D.C2 = temp2 / 2.0 / den;
+        D.C3 = 2.0 * dt / den;
+        for (int q = 0; q < p->nD; ++q) D.C4[q] = (1.0 + D.kappa[q]) * dt / den;
+        for (int q = 0; q < p->nL; ++q) {
+            D.C5[q] = p->literal ? (1.0 + D.alpha[q]) / den : (1.0 + D.alpha[q]) * dt / den;
+            D.C6[q] = D.xi[q] * dt / den;
+        }
     }
     if ((s = build_list(g, CPS_ID_DISPERSIVE, &g->dl_n, &g->d_dl_cell, &g->d_dl_seg))) return s;
     if ((s = dalloc(g, &g->d_dl_state, (size_t)g->dl_n * 3 * D.stride * g->esz))) return s;
     g->dl_on = true;
     return CPS_OK;
+}
+
+extern "C" cps_status cps_drude_init(cps_grid *g, const cps_drude_params *p)
+{
+    REQUIRE(p, CPS_E_INVALID, "cps_drude_init: NULL params");
+    cps_dl_params q;
+    memset(&q, 0, sizeof(q));
+    q.sigma = p->sigma; q.epsInf = p->epsInf;
+    q.nD = 1; q.nL = 0;
+    q.fD[0] = p->omegaP_hz; q.gD[0] = p->gamma_hz;
+    q.literal = 2;
+    return cps_dl_init(g, &q);
 }
 
 extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)

@@ -152,7 +152,13 @@ class Deck:
                 n = t["n6"]
                 f.write(f"{n[0]}\t{n[1]}\n{n[2]}\t{n[3]}\n{n[4]}\t{n[5]}\n{int(t['Nt'])}\n{int(t['cwmode'])}\n")
             lines.append(f"tfsf TF_SF.txt {int(t['k0'])}")
-        if self.dl:
+        if self.dl and int(self.dl.get("literal", 0)) == 2:
+            d = self.dl  # the single-pole Drude class's deck (Drude.cpp:29-52)
+            with open(os.path.join(path, "Drude.txt"), "w") as f:
+                f.write(f"{_f(d['epsInf'])}\tepsilon_infinity\n{_f(d['fD'][0])}\tomega_P (Hz)\n")
+                f.write(f"{_f(d['sigma'])}\tsigma\n{_f(d['gD'][0])}\tgamma (Hz)\n")
+            lines.append("drude Drude.txt")
+        elif self.dl:
             d = self.dl
             with open(os.path.join(path, "DrudeLorentz.txt"), "w") as f:
                 f.write(f"{len(d['fD'])}\tnum_of_D_poles\n{len(d['fL'])}\tnum_of_L_poles\n")
@@ -228,6 +234,21 @@ def dl_params_metal() -> dict:
                 fL=[4.0e15 / two_pi, 6.0e15 / two_pi],
                 dL=[1.0e15 / 2.0 / two_pi, 2.0e15 / 2.0 / two_pi],
                 depsL=[1.0, 0.5])
+
+
+def drude_params_metal() -> dict:
+    """A single-pole Drude metal for the reference's Drude class (Drude.cpp):
+    eps_inf 1, omega_P 1.37e16 rad/s, gamma 1e14 1/s (as Hz on the deck, the
+    class multiplies by 2 pi), conductivity 1e4 S/m."""
+    two_pi = 2.0 * PI
+    return dict(epsInf=1.0, fP=1.37e16 / two_pi, sigma=1.0e4, gamma=1.0e14 / two_pi)
+
+
+def drude_as_dl(drude: dict) -> dict:
+    """The Drude class as the engine's Drude-Lorentz module: one Drude pole, no
+    Lorentz pole, the coefficients of Drude.cpp (literal = 2)."""
+    return dict(sigma=drude["sigma"], epsInf=drude["epsInf"], fD=[drude["fP"]], gD=[drude["gamma"]],
+                fL=[], dL=[], depsL=[], literal=2)
 
 
 def gain_params_laser(pump: float = 1.0e9) -> dict:

@@ -22,6 +22,7 @@
  *   cps_pml_init .............. CPML::CPML + InitializeCPML (CPML.cpp:29-68, 231-527);
  *                               CFS_PML::CFS_PML + Initialize_PML (CFS_PML.h:33-36)
  *   cps_dl_init ............... Drude_Lorentz::Drude_Lorentz (Drude_Lorentz.cpp:30-147)
+ *   cps_drude_init ............ Drude::Drude (Drude.cpp:29-68); its EFieldUpdate is cps_op_dl
  *   cps_gain_init ............. FourLevelLaser::FourLevelLaser (FourLevelLaser.cpp:30-213)
  *   cps_tfsf_init ............. TF_SF::TF_SF (TF_SF.cpp:29-959)
  *   cps_source_add ............ the field injection of main.cpp:284-286
@@ -112,7 +113,8 @@ typedef struct cps_pml_params {
 /* Drude-Lorentz deck values (Drude_Lorentz.cpp:37-94); frequencies in Hz.
  * literal = 1 uses C1 and C5 exactly as Drude_Lorentz.cpp:96,106; 0 uses the
  * values the ADE discretisation gives (the literal C5 lacks a factor dt and is
- * unstable with any Lorentz pole). */
+ * unstable with any Lorentz pole); 2, with one Drude pole and no Lorentz pole,
+ * uses the single-pole Drude class's coefficients (Drude.cpp:56-60). */
 #define CPS_MAX_POLES 8
 typedef struct cps_dl_params {
     double sigma, epsInf;
@@ -121,6 +123,14 @@ typedef struct cps_dl_params {
     double fL[CPS_MAX_POLES], dL[CPS_MAX_POLES], depsL[CPS_MAX_POLES];
     int32_t literal;
 } cps_dl_params;
+
+/* Single-pole Drude deck values (Drude.cpp:29-52): eps_inf, plasma and
+ * collision frequencies in Hz (the class multiplies them by 2 pi) and the
+ * conductivity.  The same ID-2 cells and state as the Drude-Lorentz module,
+ * with the coefficients of Drude.cpp:56-60; one of the two per grid. */
+typedef struct cps_drude_params {
+    double epsInf, omegaP_hz, sigma, gamma_hz;
+} cps_drude_params;
 
 /* Four-level gain deck values (FourLevelLaser.cpp:37-93).  Gain sites are the
  * cells whose ID equals gain_id (the reference places them on ID==5,
@@ -189,6 +199,7 @@ CPS_API cps_status cps_mesh_rasterize(int32_t nx, int32_t ny, int32_t nz, double
 /* ---- physics modules (call after media and IDs are set) ---- */
 CPS_API cps_status cps_pml_init(cps_grid *g, const cps_pml_params *p);
 CPS_API cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p);
+CPS_API cps_status cps_drude_init(cps_grid *g, const cps_drude_params *p);
 CPS_API cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p);
 CPS_API cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p);
 /* replace the incident tables Einc/Hinc (n = Nt + 1 values each) */

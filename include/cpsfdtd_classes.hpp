@@ -1,10 +1,10 @@
 // cpsfdtd_classes.hpp -- the cpsFDTD host classes (Structure, Field,
-// BasicEFieldUpdate/BasicHFieldUpdate, CPML, CFS_PML, Drude_Lorentz,
+// BasicEFieldUpdate/BasicHFieldUpdate, CPML, CFS_PML, Drude_Lorentz, Drude,
 // FourLevelLaser, TF_SF, SphericalPort, PlainPort) with the reference's names,
 // constructors, public members and update methods, reading the same
 // resourses/*.txt decks, over the C ABI of cps_capi.h.  A main.cpp written
 // for the reference compiles against this header instead of Structure.h,
-// Fields.h, BasicFDTD.h, CPML.h, CFS_PML.h, Drude_Lorentz.h,
+// Fields.h, BasicFDTD.h, CPML.h, CFS_PML.h, Drude_Lorentz.h, Drude.h,
 // FourLevelLaser.h, TF_SF.h and Ports.h, and links with -lcpsfdtd.
 //
 // State lives on the GPU; update calls are recorded on the grid
@@ -379,6 +379,31 @@ public:
 
     double sigma = 0, epsInf = 1;
     int num_of_D_poles = 0, num_of_L_poles = 0;
+};
+
+// Drude.h:19-35: the single-pole Drude material of the ID-2 cells, deck
+// Drude.cpp:29-52 (eps_inf, omega_P and gamma in Hz, sigma); its update
+// (Drude.cpp:70-113) is the Drude-Lorentz cell update with Drude.cpp's
+// coefficients.  One of Drude and Drude_Lorentz per Structure.
+class Drude {
+public:
+    Drude(Structure &sS, const char *fileName)
+    {
+        cpsfdtd_detail::LineReader r(fileName);
+        cps_drude_params p{};
+        r.line(0) >> p.epsInf;
+        r.line(1) >> p.omegaP_hz;
+        r.line(2) >> p.sigma;
+        r.line(3) >> p.gamma_hz;
+        epsInf = p.epsInf;
+        omegaP = p.omegaP_hz * 2.0 * 3.1415926535897932384626433832795;  // Drude.cpp:40
+        sigma = p.sigma;
+        gamma = p.gamma_hz * 2.0 * 3.1415926535897932384626433832795;  // Drude.cpp:49
+        cpsfdtd_detail::check(cps_drude_init(sS.grid(), &p), "Drude");
+    }
+    void EFieldUpdate(Field &fF, Structure &) { cpsfdtd_detail::check(cps_op_dl(fF.grid()), "EFieldUpdate"); }
+
+    double epsInf = 1, omegaP = 0, sigma = 0, gamma = 0;
 };
 
 // FourLevelLaser.h:8-52: deck FourLevelLaser.cpp:37-93; gain sites are the

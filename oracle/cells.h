@@ -72,6 +72,16 @@ static void dl_coeffs(dl_t *D, double dt, double sigma, double epsInf, int nD, c
         D->gammaL[p] = (K_EPS0 * depsL[p] * omega * omega * dt * dt) / (1.0 + delta * dt);
         temp2 = temp2 + D->gammaL[p];
     }
+    if (literal == 2 && nD == 1 && nL == 0) {
+        /* the single-pole Drude class: Drude.cpp:56-60 in its own order
+         * (C1Drude, C2Drude, C3Drude are the C1, C3, C4[0] of this recursion) */
+        const double b = D->beta[0], kp = D->kappa[0];
+        D->C1 = (2 * K_EPS0 * epsInf - dt * b - sigma * dt) / (2 * K_EPS0 * epsInf + dt * b + sigma * dt);
+        D->C2 = 0.0;
+        D->C3 = (2 * dt) / (2 * K_EPS0 * epsInf + dt * b + sigma * dt);
+        D->C4[0] = ((1 + kp) * dt) / (2 * K_EPS0 * epsInf + dt * b + sigma * dt);
+        return;
+    }
     const double den = 2.0 * K_EPS0 * epsInf + sigma * dt + dt * temp1 + temp2 / 2.0;
     /* literal: C1 and C5 exactly as Drude_Lorentz.cpp:96,106.  Otherwise the
      * values the ADE discretisation gives: the E^n coefficient carries

@@ -60,7 +60,9 @@ int orc_set_ids(orc *o, const uint8_t *ids);
 int orc_pml_init(orc *o, const int32_t npml[6], double m, double malp,
                  double kapmax, double sig_ratio, double alpmax);
 /* literal = 1 takes C1 and C5 exactly as Drude_Lorentz.cpp:96,106; 0 (the
- * default of the product) takes the values the ADE discretisation gives. */
+ * default of the product) takes the values the ADE discretisation gives;
+ * 2 (one Drude pole, no Lorentz pole) is the single-pole Drude class with the
+ * coefficients of Drude.cpp:56-60 (fD = omegaP, gD = gamma in Hz). */
 int orc_dl_init(orc *o, double sigma, double epsInf,
                 int nD, const double *fD, const double *gD,
                 int nL, const double *fL, const double *dL, const double *depsL, int literal);

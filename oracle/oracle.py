@@ -264,15 +264,16 @@ def ref_bench(dk, warm, timed, threads=0, exe=None, timeout=900):
         shutil.rmtree(workdir, ignore_errors=True)
 
 
-def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, timeout=120):
-    """Run the reference's 2-D Drude_Lorentz / FourLevelLaser classes.
-    params: dict nx ny dx dy dt nsteps si sj.  Returns (Ex, Ey, Hz)."""
+def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, timeout=120):
+    """Run the reference's 2-D Drude_Lorentz / FourLevelLaser / Drude classes.
+    params: dict nx ny dx dy dt nsteps si sj; drude: dict epsInf fP sigma gamma
+    (Hz) for the single-pole Drude class.  Returns (Ex, Ey, Hz)."""
     workdir = tempfile.mkdtemp(prefix="cps_ref2d_")
     try:
         p = params
         with open(os.path.join(workdir, "params2d.txt"), "w") as f:
             f.write(f"{p['nx']} {p['ny']} {float(p['dx'])!r} {float(p['dy'])!r} {float(p['dt'])!r} {p['nsteps']} {p['si']} {p['sj']} "
-                    f"{1 if dl else 0} {1 if gain else 0} {int((dl or {}).get('literal', 0))}\n")
+                    f"{1 if dl else 0} {1 if gain else 0} {int((dl or {}).get('literal', 0))} {1 if drude else 0}\n")
         with open(os.path.join(workdir, "media2d.txt"), "w") as f:
             f.write(f"{len(media)}\n")
             for m in media:
@@ -286,6 +287,10 @@ def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, timeout=120):
                     f.write(f"{float(a)!r}\t{float(b)!r}\n")
                 for a, b, c in zip(dl["fL"], dl["dL"], dl["depsL"]):
                     f.write(f"{float(a)!r}\t{float(b)!r}\t{float(c)!r}\n")
+        if drude:
+            with open(os.path.join(workdir, "Drude.txt"), "w") as f:
+                for key in ("epsInf", "fP", "sigma", "gamma"):
+                    f.write(f"{float(drude[key])!r}\n")
         if gain:
             g = gain
             with open(os.path.join(workdir, "FourLevelLaser.txt"), "w") as f:
@@ -303,9 +308,18 @@ def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, timeout=120):
         shutil.rmtree(workdir, ignore_errors=True)
 
 
-def run_orc2d(params, media, ids2d, wave, dl=None, gain=None):
+def drude_as_dl(drude):
+    """The single-pole Drude class as the oracle's Drude-Lorentz recursion with
+    one Drude pole and the coefficients of Drude.cpp (literal = 2)."""
+    return dict(sigma=drude["sigma"], epsInf=drude["epsInf"], fD=[drude["fP"]], gD=[drude["gamma"]],
+                fL=[], dL=[], depsL=[], literal=2)
+
+
+def run_orc2d(params, media, ids2d, wave, dl=None, gain=None, drude=None):
     """The oracle's 2-D TE driver on the same problem as run_ref2d."""
     L = lib()
+    if drude:
+        dl = drude_as_dl(drude)
     p = params
     m = np.array(media, dtype=np.float64).reshape(-1, 4)
     cols = [_dp(m[:, c]) for c in range(4)]

@@ -8,7 +8,7 @@
 // TEST INFRASTRUCTURE ONLY.
 //
 // Usage: ref2d_harness <deck_dir> <out_dir>
-//   params2d.txt : nx ny dx dy dt nsteps si sj use_dl use_gain [dl_literal]
+//   params2d.txt : nx ny dx dy dt nsteps si sj use_dl use_gain [dl_literal [use_drude]]
 //   With dl_literal 0 the constructed Drude_Lorentz gets C1 and C5 overwritten
 //   with the values the ADE discretisation gives (Drude_Lorentz.cpp:96 has the
 //   wrong sign on sigma*dt + dt*sum(beta), :106 lacks a factor dt); the update
@@ -16,7 +16,8 @@
 //   media2d.txt  : n, then n lines epsR muR sig sigM
 //   ids2d.bin    : uint8 [nx+1][ny+1], j fastest
 //   wave.bin     : nsteps doubles, added to Hz[si][sj] after each H update
-//   DrudeLorentz.txt / FourLevelLaser.txt : reference-format decks
+//   DrudeLorentz.txt / FourLevelLaser.txt / Drude.txt : reference-format decks;
+//   use_drude runs the single-pole Drude class (Drude.cpp) as the E update
 #include "stdafx.h"
 #include "Constants.h"
 #include "Structure.h"
@@ -37,6 +38,7 @@
 #include "Drude_Lorentz.h"
 #undef private
 #include "FourLevelLaser.h"
+#include "Drude.h"
 
 void *operator new(std::size_t n) { void *p = calloc(n ? n : 1, 1); if (!p) throw std::bad_alloc(); return p; }
 void *operator new[](std::size_t n) { void *p = calloc(n ? n : 1, 1); if (!p) throw std::bad_alloc(); return p; }
@@ -58,12 +60,13 @@ int main(int argc, char **argv)
 {
     if (argc < 3) die("usage");
     const std::string dir = std::string(argv[1]) + "/", out = std::string(argv[2]) + "/";
-    int nx, ny, nsteps, si, sj, use_dl, use_gain, dl_literal = 1;
+    int nx, ny, nsteps, si, sj, use_dl, use_gain, dl_literal = 1, use_drude = 0;
     double dx, dy, dt;
     {
         std::ifstream p(dir + "params2d.txt");
         if (!(p >> nx >> ny >> dx >> dy >> dt >> nsteps >> si >> sj >> use_dl >> use_gain)) die("params");
         if (!(p >> dl_literal)) dl_literal = 1;
+        if (!(p >> use_drude)) use_drude = 0;
     }
     int nm;
     std::ifstream mi(dir + "media2d.txt");
@@ -104,9 +107,10 @@ int main(int argc, char **argv)
         if (!f || fread(wave.data(), sizeof(double), nsteps, f) != (size_t)nsteps) die("wave");
         fclose(f);
     }
-    std::string dlf = dir + "DrudeLorentz.txt", glf = dir + "FourLevelLaser.txt";
-    std::vector<char> dln(dlf.begin(), dlf.end()), gln(glf.begin(), glf.end());
-    dln.push_back(0); gln.push_back(0);
+    std::string dlf = dir + "DrudeLorentz.txt", glf = dir + "FourLevelLaser.txt", drf = dir + "Drude.txt";
+    std::vector<char> dln(dlf.begin(), dlf.end()), gln(glf.begin(), glf.end()), drn(drf.begin(), drf.end());
+    dln.push_back(0); gln.push_back(0); drn.push_back(0);
+    Drude *DR = use_drude ? new Drude(S, drn.data()) : nullptr;
     Drude_Lorentz *DL = use_dl ? new Drude_Lorentz(S, dln.data()) : nullptr;
     FourLevelLaser *FL = use_gain ? new FourLevelLaser(S, gln.data()) : nullptr;
     if (DL && !dl_literal) {
@@ -121,7 +125,9 @@ int main(int argc, char **argv)
                 F.Hz[i][j] = S.aH[id] * F.Hz[i][j] + S.bH[id] * (F.Ex[i][j + 1] - F.Ex[i][j]) * cy - S.bH[id] * (F.Ey[i + 1][j] - F.Ey[i][j]) * cx;
             }
         F.Hz[si][sj] = F.Hz[si][sj] + wave[n];
-        if (DL) {
+        if (DR) {
+            DR->EFieldUpdate(F, S);
+        } else if (DL) {
             DL->EFieldUpdate(F, S);
         } else {
             for (int i = 1; i < nx; ++i)

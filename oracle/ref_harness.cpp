@@ -150,7 +150,7 @@ int main(int argc, char **argv)
     if (argc < 3) die("usage: ref_harness <deck_dir> <out_dir>");
     const std::string dir = std::string(argv[1]) + "/", out = std::string(argv[2]) + "/";
     int nsteps = 0, n0 = 1, record_ports = 0, warm = -1, timed = 0, threads = 0;
-    std::string pml_file, tfsf_file, ids_file, dl_file, gain_file;
+    std::string pml_file, tfsf_file, ids_file, dl_file, gain_file, drude_file;
     int tfsf_k0 = 0, dl_literal = 0;
     std::vector<Source> sources;
     std::vector<std::pair<int, std::string>> port_files;  // 0 plain, 1 spherical
@@ -169,6 +169,7 @@ int main(int argc, char **argv)
             else if (key == "ids") s >> ids_file;
             else if (key == "dl") { s >> dl_file; if (!(s >> dl_literal)) dl_literal = 0; }
             else if (key == "gain") s >> gain_file;
+            else if (key == "drude") s >> drude_file;
             else if (key == "record_ports") s >> record_ports;
             else if (key == "bench") s >> warm >> timed;
             else if (key == "threads") s >> threads;
@@ -237,10 +238,23 @@ int main(int argc, char **argv)
     memset(&D, 0, sizeof(D));
     std::vector<int> dl_cells;
     std::vector<double> dl_state;
-    if (!dl_file.empty()) {
+    if (!dl_file.empty() || !drude_file.empty()) {
         double sigma, epsInf; int nD, nL;
         std::vector<double> fD, gD, fL, dL, de;
-        read_dl(dir + dl_file, sigma, epsInf, nD, fD, gD, nL, fL, dL, de);
+        if (!drude_file.empty()) {  // the single-pole Drude deck, Drude.cpp:29-52
+            std::ifstream f(dir + drude_file);
+            std::string line;
+            double v[4] = {0, 0, 0, 0};
+            for (int q = 0; q < 4; ++q) {
+                if (!std::getline(f, line)) die("drude deck");
+                std::istringstream(line) >> v[q];
+            }
+            epsInf = v[0]; sigma = v[2]; nD = 1; nL = 0;
+            fD = {v[1]}; gD = {v[3]}; fL = {0.0}; dL = {0.0}; de = {0.0};
+            dl_literal = 2;
+        } else {
+            read_dl(dir + dl_file, sigma, epsInf, nD, fD, gD, nL, fL, dL, de);
+        }
         dl_coeffs(&D, S.dt, sigma, epsInf, nD, fD.data(), gD.data(), nL, fL.data(), dL.data(), de.data(), dl_literal);
         D.stride = nD + 2 * nL + 1;
         for (int i = 1; i < Nx; ++i)

@@ -40,6 +40,8 @@ int main(int argc, char **argv)
         }
         std::unique_ptr<Drude_Lorentz> DL;
         if (exists(dir + "/DrudeLorentz.txt")) DL.reset(new Drude_Lorentz(S, (dir + "/DrudeLorentz.txt").c_str()));
+        std::unique_ptr<Drude> DR;
+        if (exists(dir + "/Drude.txt")) DR.reset(new Drude(S, (dir + "/Drude.txt").c_str()));
         std::unique_ptr<FourLevelLaser> FL;
         if (exists(dir + "/FourLevelLaser.txt")) FL.reset(new FourLevelLaser(S, (dir + "/FourLevelLaser.txt").c_str()));
         std::unique_ptr<TF_SF> tfsf;
@@ -58,6 +60,7 @@ int main(int argc, char **argv)
             if (pml) pml->UpdateCPMLHFields(F);
             BasicEFieldUpdate(F, S);
             if (DL) DL->EFieldUpdate(F, S);
+            if (DR) DR->EFieldUpdate(F, S);
             if (FL) {
                 FL->UpdatePolarizationDensities(F);
                 FL->UpdateElectricField(F);

@@ -68,6 +68,8 @@ def _grid2d(kind):
     ids[(ii - 26) ** 2 + (jj - 24) ** 2 <= 64] = 2
     ids[40:44, 8:12] = 4
     media = [(1, 1, 0, 0), (1, 1, 0, 0), (1, 1, 0, 0), (1, 1, 0, 0), (1, 1, 0, 0)]
+    if kind == "drude":  # the single-pole Drude class (Drude.cpp), with conductivity
+        return p, media, ids, wave, {"drude": decks.drude_params_metal()}
     dl = decks.dl_params_metal()
     if kind == "dl_literal":
         dl = dict(dl, fL=[], dL=[], depsL=[], literal=1, sigma=1e4)
@@ -75,4 +77,4 @@ def _grid2d(kind):
 
 
 CASES_2D = {"dl": lambda: _grid2d("dl"), "dl_literal": lambda: _grid2d("dl_literal"),
-            "gain": lambda: _grid2d("gain")}
+            "gain": lambda: _grid2d("gain"), "drude": lambda: _grid2d("drude")}

@@ -35,7 +35,7 @@ def test_dropin_main_builds_and_fails_loudly(tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("record", ["1", "0"])
-@pytest.mark.parametrize("case", ["dispersive", "dielectric"])
+@pytest.mark.parametrize("case", ["dispersive", "dielectric", "drude"])
 def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
     """record "1": the classes' calls run as fused steps (the default);
     "0": routine by routine."""
@@ -43,6 +43,9 @@ def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
     exe = _build(tmp_path)
     if case == "dispersive":
         dk = decks.config2(n=32, steps=40, nfreq=2)
+    elif case == "drude":  # the single-pole Drude class (Drude.txt deck)
+        dk = decks.config2(n=32, steps=40, nfreq=2)
+        dk.dl = decks.drude_as_dl(decks.drude_params_metal())
     else:
         dk = decks.config1(n=28, steps=40)
         dk.sources = []  # point sources are main.cpp code, not a class: drive it with a TF/SF beam instead

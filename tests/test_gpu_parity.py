@@ -27,7 +27,15 @@ def _setup(dk, oracle_mod):
     return ids, pts, o
 
 
+def _c2_drude():
+    """The dispersive deck with the single-pole Drude class (Drude.cpp) on its spheres."""
+    dk = decks.config2(n=40, steps=100, nfreq=4)
+    dk.dl = decks.drude_as_dl(decks.drude_params_metal())
+    return dk
+
+
 CASES = {"c1": lambda: decks.config1(n=32, steps=120),
+         "c2_drude": _c2_drude,
          "c2": lambda: decks.config2(n=48, steps=100, nfreq=8),
          "c2_cw": gc.c2_cw,
          "c3": lambda: decks.config3(n=40, steps=100, nfreq=4),
@@ -124,3 +132,23 @@ def test_tma_and_register_sweeps_agree(prec):
     for other in out[1:]:
         for a, b in zip(out[0], other):
             assert rel_l2(a, b) < tol
+
+
+def test_drude_entry_point_equals_dl_form():
+    """cps_drude_init (the Drude class's constructor) sets up exactly the
+    Drude-Lorentz module in its single-pole Drude form."""
+    import cpsfdtd_b200 as cps
+    dk = _c2_drude()
+    a = cps.Grid.from_deck(dk, cps.FP64)
+    dl = dk.dl
+    dk.dl = None
+    b = cps.Grid.from_deck(dk, cps.FP64)
+    dr = decks.drude_params_metal()
+    with pytest.raises(cps.CpsError):
+        b.drude_init(dict(dr, epsInf=-1.0))
+    b.drude_init(dr)
+    dk.dl = dl
+    a.step(30, cps.FUSED)
+    b.step(30, cps.FUSED)
+    for c in range(6):
+        assert np.array_equal(a.field(c), b.field(c))

@@ -74,3 +74,16 @@ def test_dl_kat_is_stable_and_dispersive(oracle_mod):
     assert np.isfinite(Ex).all() and np.abs(Ex).max() < 10
     plain = oracle_mod.run_orc2d(p, media, ids, wave, dl=None)
     assert np.abs(Ex - plain[0]).max() > 1e-3 * np.abs(plain[0]).max()
+
+
+def test_drude_kat_is_dispersive_and_lossy(oracle_mod):
+    """The single-pole Drude KAT (the reference's Drude class) differs from the
+    free-space run and from the same pole without the Drude class's C1."""
+    p, media, ids, wave, kw = gc.CASES_2D["drude"]()
+    Ex, Ey, Hz = oracle_mod.run_orc2d(p, media, ids, wave, **kw)
+    assert np.isfinite(Ex).all()
+    plain = oracle_mod.run_orc2d(p, media, ids, wave)
+    assert np.abs(Ex - plain[0]).max() > 1e-3 * np.abs(plain[0]).max()
+    literal_dl = dict(oracle_mod.drude_as_dl(kw["drude"]), literal=1)
+    other = oracle_mod.run_orc2d(p, media, ids, wave, dl=literal_dl)
+    assert np.abs(Ex - other[0]).max() > 0
