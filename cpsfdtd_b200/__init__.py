@@ -60,6 +60,12 @@ class DrudeParams(C.Structure):
     _fields_ = [("epsInf", C.c_double), ("omegaP_hz", C.c_double), ("sigma", C.c_double), ("gamma_hz", C.c_double)]
 
 
+class ThreeParams(C.Structure):
+    _fields_ = [("gain_id", C.c_int32), ("lambda_a", C.c_double), ("lambda_b", C.c_double),
+                ("gamma_a", C.c_double), ("gamma_b", C.c_double), ("t20", C.c_double), ("t21", C.c_double),
+                ("t10", C.c_double), ("N_0", C.c_double), ("N_1", C.c_double), ("literal", C.c_int32)]
+
+
 class GainParams(C.Structure):
     _fields_ = [("gain_id", C.c_int32), ("lambda_a", C.c_double), ("lambda_b", C.c_double),
                 ("gamma_a", C.c_double), ("gamma_b", C.c_double), ("t30", C.c_double), ("t32", C.c_double),
@@ -105,6 +111,10 @@ def lib():
             "cps_pml_init": ([P, C.POINTER(PmlParams)], I32),
             "cps_dl_init": ([P, C.POINTER(DlParams)], I32),
             "cps_drude_init": ([P, C.POINTER(DrudeParams)], I32),
+            "cps_three_init": ([P, C.POINTER(ThreeParams)], I32),
+            "cps_three_populations": ([P, dp, C.POINTER(I64)], I32),
+            "cps_op_three_polarization": ([P], I32), "cps_op_three_efield": ([P], I32),
+            "cps_op_three_populations": ([P], I32),
             "cps_gain_init": ([P, C.POINTER(GainParams)], I32),
             "cps_tfsf_init": ([P, C.POINTER(TfsfParams)], I32),
             "cps_tfsf_set_tables": ([P, I32, dp, dp], I32), "cps_tfsf_get_tables": ([P, I32, dp, dp], I32),
@@ -235,6 +245,8 @@ class Grid:
             g.dl_init(dk.dl)
         if dk.gain:
             g.gain_init(dk.gain)
+        if getattr(dk, "three", None):
+            g.three_init(dk.three)
         if dk.tfsf:
             g.tfsf_init(dk.tfsf_abi())
         for comp, i, j, k, wave in dk.sources:
@@ -278,6 +290,21 @@ class Grid:
         """The single-pole Drude class (Drude.cpp): dict epsInf fP sigma gamma (Hz)."""
         pp = DrudeParams(d["epsInf"], d["fP"], d["sigma"], d["gamma"])
         _check(self.L.cps_drude_init(self.h, C.byref(pp)))
+
+    def three_init(self, t):
+        """The three-level gain class (ThreeLevel.cpp): dict lambda_a lambda_b gamma_a
+        gamma_b t20 t21 t10 N_0 [N_1 gain_id literal]."""
+        pp = ThreeParams(int(t.get("gain_id", 5)), t["lambda_a"], t["lambda_b"], t["gamma_a"], t["gamma_b"],
+                         t["t20"], t["t21"], t["t10"], t["N_0"], t.get("N_1", 0.0), int(t.get("literal", 0)))
+        _check(self.L.cps_three_init(self.h, C.byref(pp)))
+
+    def three_populations(self):
+        """[ncells][3] N0 N1 N2 of the three-level sites, cells in (i,j,k) order"""
+        n = C.c_int64()
+        _check(self.L.cps_three_populations(self.h, None, C.byref(n)))
+        out = np.empty((n.value, 3))
+        _check(self.L.cps_three_populations(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)))
+        return out
 
     def gain_init(self, g):
         pp = GainParams(int(g.get("gain_id", 5)), g["lambda_a"], g["lambda_b"], g["gamma_a"], g["gamma_b"],

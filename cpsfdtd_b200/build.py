@@ -34,6 +34,7 @@ SOURCES = {
     "kernels_ports.cu": [],
     "kernels_batch.cu": [],
     "kernels_step.cu": [],
+    "kernels_three.cu": ["--fmad=false"],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
     "noalloc.cu": [],

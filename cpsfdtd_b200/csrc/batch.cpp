@@ -533,6 +533,7 @@ extern "C" cps_status cps_batch_add(cps_batch *b, cps_grid *g)
     REQUIRE(b && g, CPS_E_INVALID, "cps_batch_add: NULL argument");
     REQUIRE(g->fp32 == b->fp32, CPS_E_INVALID, "cps_batch_add: grid precision differs from the batch's");
     REQUIRE(g->nmedia > 0 && g->ids_set, CPS_E_STATE, "cps_batch_add: grid media and IDs must be set first");
+    REQUIRE(!g->three_on, CPS_E_INVALID, "cps_batch_add: grids with the three-level gain are stepped one at a time");
     REQUIRE(std::find(b->grids.begin(), b->grids.end(), g) == b->grids.end(), CPS_E_INVALID,
             "cps_batch_add: grid is already in the batch");
     REQUIRE(g->d.px >= 64 && g->d.ny + 1 >= 9 && g->d.nz >= 2, CPS_E_INVALID,

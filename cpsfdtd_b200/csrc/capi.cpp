@@ -591,6 +591,13 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
                 launch_gain<T>(f, G, 1, g->stream);
                 launch_gain<T>(f, G, 2, g->stream);
             }
+            if (g->three_on) {
+                const ThreeView tv = three_view(g);
+                launch_three<T>(f, tv, 0, g->stream);
+                launch_three<T>(f, tv, 1, g->stream);
+                launch_three<T>(f, tv, 2, g->stream);
+                g->launches += 3;
+            }
             op_inject<T>(g, 0, (double)n, CPS_FACE_ALL);
             op_sources<T>(g, (int)n);
             if (g->pml_on) launch_e_pml<T>(f, p, g->stream);
@@ -618,6 +625,10 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
                 launch_dl_cells_step<T>(field_view<T>(g), field_view_alt<T>(g), pml_view<T>(g), D, g->stream);
                 g->launches++;
             }
+            if (g->three_on) {
+                launch_three<T>(field_view<T>(g), three_view(g), 3, g->stream);
+                g->launches++;
+            }
             if (timed) {
                 cudaEventRecord(g->ev[g->ev_used + 3], g->stream);
                 g->ev_used += 4;
@@ -635,6 +646,10 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             if (timed) cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
             if (use_tma) launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream);
             else launch_e_fused<T>(f, p, D, G, g->shape, g->stream);
+            if (g->three_on) {
+                launch_three<T>(f, three_view(g), 3, g->stream);
+                g->launches++;
+            }
             if (timed) {
                 cudaEventRecord(g->ev[g->ev_used + 3], g->stream);
                 g->ev_used += 4;
@@ -1028,6 +1043,59 @@ extern "C" cps_status cps_drude_init(cps_grid *g, const cps_drude_params *p)
     return cps_dl_init(g, &q);
 }
 
+extern "C" cps_status cps_three_init(cps_grid *g, const cps_three_params *p)
+{
+    cps_status s = need_setup(g);
+    if (s) return s;
+    FLUSH_RECORDED(g);
+    REQUIRE(p, CPS_E_INVALID, "cps_three_init: NULL params");
+    REQUIRE(!g->three_on, CPS_E_STATE, "cps_three_init: already initialised");
+    REQUIRE(!g->gain_on, CPS_E_STATE, "cps_three_init: the grid already has the four-level gain");
+    REQUIRE(p->gain_id >= 0 && p->gain_id <= 255 && p->gain_id != CPS_ID_DISPERSIVE && p->gain_id != CPS_ID_PEC,
+            CPS_E_INVALID, "cps_three_init: gain_id must be a plain medium");
+    REQUIRE(p->lambda_a > 0 && p->lambda_b > 0 && p->t20 > 0 && p->t21 > 0 && p->t10 > 0 && p->N_0 > 0,
+            CPS_E_INVALID, "cps_three_init: wavelengths, lifetimes and N_0 must be positive");
+    REQUIRE(p->literal == 0 || p->literal == 1, CPS_E_INVALID, "cps_three_init: literal must be 0 or 1");
+    const double dt = g->desc.dt;
+    ThreeCoef &K = g->tc;
+    // ThreeLevel.cpp:96-119, :208
+    const double omega_a = 2.0 * kPi * kC / p->lambda_a, omega_b = 2.0 * kPi * kC / p->lambda_b;
+    const double ga = p->gamma_a, gb = p->gamma_b, t20 = p->t20, t21 = p->t21, t10 = p->t10;
+    if (p->literal) {
+        K.CPa1 = 2 / ((dt * dt + omega_a * omega_a) * (1 / (dt * dt) + ga / (2 * dt)));
+        K.CPa2 = (2 / (dt * dt) + 1 / (2 * dt)) / (1 / (dt * dt) + ga / (2 * dt));
+        K.CPb1 = 2 / ((dt * dt + omega_b * omega_b) * (1 / (dt * dt) + gb / (2 * dt)));
+        K.CPb2 = (2 / (dt * dt) + 1 / (2 * dt)) / (1 / (dt * dt) + gb / (2 * dt));
+    } else {
+        K.CPa1 = (2 / (dt * dt) - omega_a * omega_a) / (1 / (dt * dt) + ga / (2 * dt));
+        K.CPa2 = (ga / (2 * dt) - 1 / (dt * dt)) / (1 / (dt * dt) + ga / (2 * dt));
+        K.CPb1 = (2 / (dt * dt) - omega_b * omega_b) / (1 / (dt * dt) + gb / (2 * dt));
+        K.CPb2 = (gb / (2 * dt) - 1 / (dt * dt)) / (1 / (dt * dt) + gb / (2 * dt));
+    }
+    K.CPa3 = (kQe * kQe / kMe) / (1 / (dt * dt) + ga / (2 * dt)) / p->N_0;
+    K.CPb3 = (kQe * kQe / kMe) / (1 / (dt * dt) + gb / (2 * dt)) / p->N_0;
+    K.CN2N2 = (1.0 / dt - 1.0 / (2.0 * t20) - 1.0 / (2.0 * t21)) / (1.0 / dt + 1.0 / (2.0 * t20) + 1.0 / (2.0 * t21));
+    K.CN2E = (1.0 / (2.0 * dt * kHPlanck * omega_a / 2.0 / kPi)) / (1.0 / dt + 1.0 / (2.0 * t20) + 1.0 / (2.0 * t21));
+    K.CN1N1 = (1.0 / dt - 1.0 / (2.0 * t10)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    K.CN1N2 = (1.0 / (2.0 * t21)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    K.CN1E = (1.0 / (2.0 * dt * kHPlanck * omega_b / 2.0 / kPi)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    K.CN0N1 = dt / (2.0 * t10);
+    K.CN0N2 = dt / (2.0 * t20);
+    K.CN0Ea = 1.0 / (2.0 * kHPlanck * omega_a / 2.0 / kPi);
+    K.CN0Eb = 1.0 / (2.0 * kHPlanck * omega_b / 2.0 / kPi);
+    K.CN0Ebx = p->literal ? K.CN0Ea : K.CN0Eb;
+    K.CEP = 1.0 / dt / kEps0;
+    g->three_id = p->gain_id;
+    g->three_N0 = p->N_0;
+    if ((s = build_list(g, p->gain_id, &g->t_n, &g->d_t_cell, &g->d_t_seg))) return s;
+    if ((s = dalloc(g, (void **)&g->d_t_state, (size_t)g->t_n * kThreeWords * sizeof(double)))) return s;
+    g->three_on = true;
+    launch_three_init(three_view(g), p->N_0, g->stream);
+    g->launches++;
+    CK(cudaGetLastError());
+    return CPS_OK;
+}
+
 extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
 {
     cps_status s = need_setup(g);
@@ -1035,6 +1103,7 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     FLUSH_RECORDED(g);
     REQUIRE(p, CPS_E_INVALID, "cps_gain_init: NULL params");
     REQUIRE(!g->gain_on, CPS_E_STATE, "cps_gain_init: already initialised");
+    REQUIRE(!g->three_on, CPS_E_STATE, "cps_gain_init: the grid already has the three-level gain");
     REQUIRE(p->gain_id >= 0 && p->gain_id < 256 && p->gain_id != CPS_ID_DISPERSIVE && p->gain_id != CPS_ID_PEC,
             CPS_E_INVALID, "cps_gain_init: gain_id must be a plain medium (not 2 or 4)");
     REQUIRE(p->lambda_a > 0 && p->lambda_b > 0 && p->t30 > 0 && p->t32 > 0 && p->t21 > 0 && p->t10 > 0 && p->N_0 > 0,
@@ -1486,16 +1555,20 @@ extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
 namespace cps {
 namespace {
 
-bool absorbed_kind(int k) { return k == kOpHPml || k == kOpEPml || k == kOpDl || (k >= kOpGainP && k <= kOpGainN); }
+bool absorbed_kind(int k)
+{
+    return k == kOpHPml || k == kOpEPml || k == kOpDl || (k >= kOpGainP && k <= kOpGainN) ||
+           (k >= kOpThreeP && k <= kOpThreeN);
+}
 
 // Whether `ops` is a prefix (full = false) or a whole step (full = true) that
 // the fused sweeps reproduce.
 bool fusable(const cps_grid *g, const std::vector<RecOp> &ops, bool full)
 {
     int phase = 0;  // 0 start, 1 H terms, 2 dispersive E terms, 3 additive E terms, 4 ports
-    int hpml = 0, epml = 0, dl = 0, gain = 0;
+    int hpml = 0, epml = 0, dl = 0, gain = 0, three = 0;
     std::vector<char> seen(g->ports.size(), 0);
-    const int want_dl = g->dl_on ? 1 : 0, want_gain = g->gain_on ? 3 : 0;
+    const int want_dl = g->dl_on ? 1 : 0, want_gain = g->gain_on ? 3 : 0, want_three = g->three_on ? 3 : 0;
     for (const RecOp &o : ops) {
         switch (o.kind) {
         case kOpHBulk:
@@ -1521,11 +1594,17 @@ bool fusable(const cps_grid *g, const std::vector<RecOp> &ops, bool full)
             if (phase != 2 || gain != o.kind - kOpGainP) return false;
             ++gain;
             break;
+        case kOpThreeP:
+        case kOpThreeE:
+        case kOpThreeN:
+            if (phase != 2 || three != o.kind - kOpThreeP) return false;
+            ++three;
+            break;
         case kOpTfsfE:
         case kOpSrc:
         case kOpEPml:
             if (phase == 2) {
-                if (dl != want_dl || gain != want_gain) return false;
+                if (dl != want_dl || gain != want_gain || three != want_three) return false;
                 phase = 3;
             }
             if (phase != 3) return false;
@@ -1533,7 +1612,7 @@ bool fusable(const cps_grid *g, const std::vector<RecOp> &ops, bool full)
             break;
         case kOpPort:
             if (phase < 2) return false;
-            if (phase == 2 && (dl != want_dl || gain != want_gain)) return false;
+            if (phase == 2 && (dl != want_dl || gain != want_gain || three != want_three)) return false;
             phase = 4;
             if (seen[o.port]++) return false;
             break;
@@ -1543,7 +1622,8 @@ bool fusable(const cps_grid *g, const std::vector<RecOp> &ops, bool full)
     }
     if (!full) return true;
     const int want_pml = g->pml_on ? 1 : 0;
-    return phase >= 2 && hpml == want_pml && epml == want_pml && dl == want_dl && gain == want_gain;
+    return phase >= 2 && hpml == want_pml && epml == want_pml && dl == want_dl && gain == want_gain &&
+           three == want_three;
 }
 
 // one routine alone on the grid's stream
@@ -1560,6 +1640,9 @@ cps_status run_op_T(cps_grid *g, const RecOp &o)
     case kOpGainP:
     case kOpGainE:
     case kOpGainN: launch_gain<T>(f, gain_view<T>(g), o.kind - kOpGainP, g->stream); g->launches++; break;
+    case kOpThreeP:
+    case kOpThreeE:
+    case kOpThreeN: launch_three<T>(f, three_view(g), o.kind - kOpThreeP, g->stream); g->launches++; break;
     case kOpTfsfH: op_inject<T>(g, 1, (double)o.n, o.mask); break;
     case kOpTfsfE: op_inject<T>(g, 0, (double)o.n, o.mask); break;
     case kOpSrc: {
@@ -1605,6 +1688,10 @@ cps_status run_fused_T(cps_grid *g, const std::vector<RecOp> &ops)
             if (use_tma) launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream);
             else launch_e_fused<T>(f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->stream);
             g->launches++;
+            if (g->three_on) {
+                launch_three<T>(f, three_view(g), 3, g->stream);
+                g->launches++;
+            }
             break;
         case kOpTfsfH: op_inject<T>(g, 1, (double)o.n, o.mask); break;
         case kOpTfsfE: op_inject<T>(g, 0, (double)o.n, o.mask); break;
@@ -1727,6 +1814,21 @@ extern "C" cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask)
     return submit_op(g, {kOpTfsfE, n, 0, face_mask});
 }
 extern "C" cps_status cps_op_sources(cps_grid *g, int32_t n) { return submit_op(g, {kOpSrc, n, 0, 0}); }
+extern "C" cps_status cps_op_three_polarization(cps_grid *g)
+{
+    if (g && !g->three_on) { set_error("three-level gain not initialised"); return CPS_E_STATE; }
+    return submit_op(g, {kOpThreeP, 0, 0, 0});
+}
+extern "C" cps_status cps_op_three_efield(cps_grid *g)
+{
+    if (g && !g->three_on) { set_error("three-level gain not initialised"); return CPS_E_STATE; }
+    return submit_op(g, {kOpThreeE, 0, 0, 0});
+}
+extern "C" cps_status cps_op_three_populations(cps_grid *g)
+{
+    if (g && !g->three_on) { set_error("three-level gain not initialised"); return CPS_E_STATE; }
+    return submit_op(g, {kOpThreeN, 0, 0, 0});
+}
 extern "C" cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n)
 {
     if (g && (port_id < 0 || port_id >= (int)g->ports.size())) { set_error("no such port"); return CPS_E_NOTFOUND; }
@@ -1813,6 +1915,7 @@ extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
         cps_status s = gain_state_init(g);
         if (s) return s;
     }
+    if (g->three_on) launch_three_init(three_view(g), g->three_N0, g->stream);
     for (PortState &P : g->ports) {
         P.fill = 0;
         P.last_slot = -1;
@@ -1881,6 +1984,34 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
         }
         for (int q = 0; q < 4; ++q) out[r * 4 + q] = N[q];
     }
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_three_populations(cps_grid *g, double *out, int64_t *ncells)
+{
+    REQUIRE(g && ncells, CPS_E_INVALID, "NULL argument");
+    REQUIRE(g->three_on, CPS_E_STATE, "three-level gain not initialised");
+    FLUSH_RECORDED(g);
+    *ncells = g->t_n;
+    if (!out) return CPS_OK;
+    const int64_t n = g->t_n;
+    std::vector<double> st((size_t)n * 3);
+    std::vector<int64_t> cells(n);
+    CK(cudaMemcpyAsync(st.data(), g->d_t_state + (size_t)21 * n, (size_t)n * 3 * sizeof(double),
+                       cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaMemcpyAsync(cells.data(), g->d_t_cell, n * sizeof(int64_t), cudaMemcpyDeviceToHost, g->stream));
+    CK(cudaStreamSynchronize(g->stream));
+    // device list is in device order (k, j, i); report in (i, j, k) order
+    std::vector<std::pair<int64_t, int64_t>> ord(n);
+    const Dims &d = g->d;
+    for (int64_t c = 0; c < n; ++c) {
+        const int64_t q = cells[c];
+        const int k = (int)(q / d.pxy), j = (int)((q - k * d.pxy) / d.px), i = (int)(q - k * d.pxy - (int64_t)j * d.px);
+        ord[c] = {((int64_t)i * (d.ny + 1) + j) * (d.nz + 1) + k, c};
+    }
+    std::sort(ord.begin(), ord.end());
+    for (int64_t r = 0; r < n; ++r)
+        for (int q = 0; q < 3; ++q) out[r * 3 + q] = st[(size_t)q * n + ord[r].second];
     return CPS_OK;
 }
 

@@ -31,6 +31,8 @@ constexpr double kC = 2.99792458E8;
 constexpr double kHPlanck = 6.62607004081E-34;
 constexpr double kMu0 = 1.2566370614E-6;
 constexpr double kEps0 = 8.8541878176E-12;
+constexpr double kQe = -1.602176565E-19;  // electron charge
+constexpr double kMe = 9.10938215E-31;    // electron mass
 
 // row width of an x-slab psi array ([k][j][s], s = 0..np): np+1 rounded up to
 // 32 words so every row starts on a 128-byte line
@@ -140,6 +142,22 @@ struct GainView {
     GainCoef c;
 };
 
+// --- three-level gain (ThreeLevel.cpp): FP64 state on both precisions (its
+// polarisation is of order 1e-40 of E), SoA [word][site]: Pa[3] Pa1[3] Pa2[3]
+// Pb[3] Pb1[3] Pb2[3] E1[3] N0 N1 N2 N1_1 N2_1
+constexpr int kThreeWords = 26;
+struct ThreeCoef {
+    double CPa1, CPa2, CPa3, CPb1, CPb2, CPb3, CEP;
+    double CN2N2, CN2E, CN1N1, CN1N2, CN1E, CN0N2, CN0N1, CN0Ea, CN0Eb, CN0Ebx;
+};
+struct ThreeView {
+    int on;
+    int64_t ncell;
+    const int64_t *cell;  // sorted linear indices
+    double *state;        // [word][ncell]
+    ThreeCoef c;
+};
+
 // ------------------------------------------------------------ launchers
 // Plain path: one kernel per reference routine (kernels_plain.cu, built
 // without FMA contraction so FP64 results follow the reference roundings).
@@ -149,6 +167,10 @@ template <typename T> void launch_h_pml(const FieldView<T> &f, const PmlView<T> 
 template <typename T> void launch_e_pml(const FieldView<T> &f, const PmlView<T> &p, cudaStream_t s);
 template <typename T> void launch_dl(const FieldView<T> &f, const DlView<T> &d, cudaStream_t s);
 template <typename T> void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStream_t s);
+// three-level gain sites: which 0 polarisation, 1 E field, 2 populations, 3 all
+// three in order (kernels_three.cu, no FMA contraction); init: zero state, N0 = N_0
+template <typename T> void launch_three(const FieldView<T> &f, const ThreeView &t, int which, cudaStream_t s);
+void launch_three_init(const ThreeView &t, double N_0, cudaStream_t s);
 template <typename T>
 void launch_inject(const FieldView<T> &f, const InjTarget *tg, int ntarget, const InjContrib *ct,
                    const T *table, int Nt, double n, uint32_t face_mask, cudaStream_t s);

@@ -49,7 +49,7 @@ struct PortState {
 
 // one recorded per-routine call (cps_op_*), kept until the recorder flushes
 enum RecKind { kOpHBulk, kOpEBulk, kOpHPml, kOpEPml, kOpDl, kOpGainP, kOpGainE, kOpGainN, kOpTfsfH, kOpTfsfE,
-               kOpSrc, kOpPort };
+               kOpSrc, kOpPort, kOpThreeP, kOpThreeE, kOpThreeN };
 struct RecOp {
     int kind;
     int32_t n;      // step index (TF/SF, sources, ports)
@@ -115,6 +115,15 @@ struct cps_grid {
     int32_t *d_g_seg = nullptr;
     uint2 *d_g_segm = nullptr;
     void *d_g_state = nullptr;
+    // three-level gain (FP64 state on both precisions)
+    bool three_on = false;
+    cps::ThreeCoef tc{};
+    int three_id = 5;
+    double three_N0 = 0.0;
+    int64_t t_n = 0;
+    int64_t *d_t_cell = nullptr;
+    int32_t *d_t_seg = nullptr;
+    double *d_t_state = nullptr;
     // TF/SF
     bool tfsf_on = false;
     cps_tfsf_params tp{};
@@ -309,6 +318,16 @@ inline GainView<T> gain_view(const cps_grid *g)
     if (!g->gain_on) return v;
     v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg; v.segm = g->d_g_segm;
     v.state = (T *)g->d_g_state; v.c = g->gc;
+    return v;
+}
+
+inline ThreeView three_view(const cps_grid *g)
+{
+    ThreeView v;
+    memset(&v, 0, sizeof(v));
+    v.on = g->three_on;
+    if (!g->three_on) return v;
+    v.ncell = g->t_n; v.cell = g->d_t_cell; v.state = g->d_t_state; v.c = g->tc;
     return v;
 }
 

@@ -87,6 +87,7 @@ class Deck:
     pml: Optional[dict] = None
     dl: Optional[dict] = None
     gain: Optional[dict] = None
+    three: Optional[dict] = None       # three-level gain (ThreeLevel.cpp), one of gain/three
     tfsf: Optional[dict] = None
     sources: list = field(default_factory=list)
     ports: list = field(default_factory=list)
@@ -177,6 +178,14 @@ class Deck:
                 f.write("0\tN_1\n")
                 f.write(f"{_f(g.get('pump', 0.0))}\tpump rate (1/s)\n")
             lines.append("gain FourLevelLaser.txt")
+        if self.three:
+            t3 = self.three  # ThreeLevel.cpp:37-84, "cells" placement
+            with open(os.path.join(path, "ThreeLevel.txt"), "w") as f:
+                f.write("cells\tdistribution\n0\tnum of sources\n0\t0\n0\t0\n")
+                for key in ("lambda_a", "lambda_b", "gamma_a", "gamma_b", "t20", "t21", "t10", "N_0"):
+                    f.write(f"{_f(t3[key])}\t{key}\n")
+                f.write("0\tN_1\n")
+            lines.append(f"three ThreeLevel.txt {int(t3.get('literal', 0))}")
         for n, (comp, i, j, k, wave) in enumerate(self.sources):
             wf = f"source{n}.bin"
             np.ascontiguousarray(wave, dtype=np.float64).tofile(os.path.join(path, wf))
@@ -234,6 +243,15 @@ def dl_params_metal() -> dict:
                 fL=[4.0e15 / two_pi, 6.0e15 / two_pi],
                 dL=[1.0e15 / 2.0 / two_pi, 2.0e15 / 2.0 / two_pi],
                 depsL=[1.0, 0.5])
+
+
+def three_params_laser(literal: int = 0) -> dict:
+    """Three-level gain on the ID-5 cells (ThreeLevel.cpp deck values):
+    transitions at 600 nm (a, 2->0) and 450 nm (b, 1->0), linewidths 2e13 Hz,
+    lifetimes t20 1 ps, t21 100 fs, t10 300 ps, density 5e23 m^-3.  literal = 1
+    takes the reference's coefficients as written (unstable oscillators)."""
+    return dict(gain_id=5, lambda_a=600e-9, lambda_b=450e-9, gamma_a=2e13, gamma_b=2e13,
+                t20=1e-12, t21=100e-15, t10=300e-12, N_0=5e23, literal=literal)
 
 
 def drude_params_metal() -> dict:

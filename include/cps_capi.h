@@ -36,6 +36,9 @@
  *   cps_op_gain_polarization .. FourLevelLaser::UpdatePolarizationDensities (FourLevelLaser.cpp:270-298)
  *   cps_op_gain_efield ........ FourLevelLaser::UpdateElectricField (FourLevelLaser.cpp:300-308)
  *   cps_op_gain_populations ... FourLevelLaser::UpdateStatesPopulations (FourLevelLaser.cpp:310-325)
+ *   cps_three_init ............ ThreeLevel::ThreeLevel (ThreeLevel.cpp:29-209)
+ *   cps_op_three_* ............ ThreeLevel::UpdatePolarizationDensities / UpdateElectricField /
+ *                               UpdateStatesPopulations (ThreeLevel.cpp:216-266), 3-D form
  *   cps_op_tfsf_h / tfsf_e .... TF_SF::UpdateHField / UpdateEField and the face variants
  *                               (TF_SF.cpp:1201-1410, 988-1199)
  *   cps_op_port_sample ........ SphericalPort/PlainPort::Update_Fields_on_Port (Ports.cpp:88-99, 342-353)
@@ -144,6 +147,23 @@ typedef struct cps_gain_params {
     double pump_rate;
 } cps_gain_params;
 
+/* Three-level gain deck values (ThreeLevel.cpp:37-84), "cells" placement on
+ * the cells of ID gain_id (the reference's "random" placement compares a char
+ * array with a literal and is never taken).  literal = 1 takes the reference's
+ * coefficients as written (ThreeLevel.cpp:100-119: its oscillator coefficients
+ * make the polarisation double every two steps, and the N0 update applies
+ * CN0Ea to the Pbx term); 0 uses the Lorentz-oscillator discretisation
+ * (2/dt^2 - w^2)/(1/dt^2 + g/2dt), (g/2dt - 1/dt^2)/(1/dt^2 + g/2dt) and CN0Eb
+ * on every b term.  N_1 is read by the reference and unused.  One of the
+ * four-level and three-level modules per grid. */
+typedef struct cps_three_params {
+    int32_t gain_id;
+    double lambda_a, lambda_b, gamma_a, gamma_b;
+    double t20, t21, t10;
+    double N_0, N_1;
+    int32_t literal;
+} cps_three_params;
+
 /* TF/SF deck values (TF_SF.cpp:35-97, 898-907).  i0 = xs/dx and j0 = ys/dy
  * (truncated), z0 = zs/dz as the reference sets it (TF_SF.cpp:55-57), k0 the
  * beam-centre plane (TF_SF.h:65; the reference never assigns it).  Angles in
@@ -201,6 +221,7 @@ CPS_API cps_status cps_pml_init(cps_grid *g, const cps_pml_params *p);
 CPS_API cps_status cps_dl_init(cps_grid *g, const cps_dl_params *p);
 CPS_API cps_status cps_drude_init(cps_grid *g, const cps_drude_params *p);
 CPS_API cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p);
+CPS_API cps_status cps_three_init(cps_grid *g, const cps_three_params *p);
 CPS_API cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p);
 /* replace the incident tables Einc/Hinc (n = Nt + 1 values each) */
 CPS_API cps_status cps_tfsf_set_tables(cps_grid *g, int32_t n, const double *einc, const double *hinc);
@@ -255,6 +276,9 @@ CPS_API cps_status cps_op_tfsf_h(cps_grid *g, int32_t n, uint32_t face_mask);
 CPS_API cps_status cps_op_tfsf_e(cps_grid *g, int32_t n, uint32_t face_mask);
 CPS_API cps_status cps_op_sources(cps_grid *g, int32_t n);
 CPS_API cps_status cps_op_port_sample(cps_grid *g, int32_t port_id, int32_t n);
+CPS_API cps_status cps_op_three_polarization(cps_grid *g);
+CPS_API cps_status cps_op_three_efield(cps_grid *g);
+CPS_API cps_status cps_op_three_populations(cps_grid *g);
 
 /* Record-and-fuse for the calls above (main.cpp:264-330 calls one routine per
  * term each step).  With recording on, cps_op_* calls are validated and queued;
@@ -286,6 +310,8 @@ CPS_API cps_status cps_grid_reset(cps_grid *g, int64_t n0);
 CPS_API cps_status cps_grid_check_finite(cps_grid *g, int64_t *nonfinite);
 /* FP64 gain populations, [ncells][4] N0..N3, cells in (i,j,k) order */
 CPS_API cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *ncells);
+/* three-level populations, [ncells][3] N0 N1 N2, cells in (i,j,k) order */
+CPS_API cps_status cps_three_populations(cps_grid *g, double *out, int64_t *ncells);
 /* number of kernel launches this grid has enqueued since creation */
 CPS_API cps_status cps_grid_launch_count(const cps_grid *g, int64_t *launches);
 /* fold the port samples still held in the rings into the DFT accumulators

@@ -1,11 +1,11 @@
 // cpsfdtd_classes.hpp -- the cpsFDTD host classes (Structure, Field,
 // BasicEFieldUpdate/BasicHFieldUpdate, CPML, CFS_PML, Drude_Lorentz, Drude,
-// FourLevelLaser, TF_SF, SphericalPort, PlainPort) with the reference's names,
+// FourLevelLaser, ThreeLevel, TF_SF, SphericalPort, PlainPort) with the reference's names,
 // constructors, public members and update methods, reading the same
 // resourses/*.txt decks, over the C ABI of cps_capi.h.  A main.cpp written
 // for the reference compiles against this header instead of Structure.h,
 // Fields.h, BasicFDTD.h, CPML.h, CFS_PML.h, Drude_Lorentz.h, Drude.h,
-// FourLevelLaser.h, TF_SF.h and Ports.h, and links with -lcpsfdtd.
+// FourLevelLaser.h, ThreeLevel.h, TF_SF.h and Ports.h, and links with -lcpsfdtd.
 //
 // State lives on the GPU; update calls are recorded on the grid
 // (cps_grid_set_record): a step made in main.cpp's order runs as the two
@@ -404,6 +404,69 @@ public:
     void EFieldUpdate(Field &fF, Structure &) { cpsfdtd_detail::check(cps_op_dl(fF.grid()), "EFieldUpdate"); }
 
     double epsInf = 1, omegaP = 0, sigma = 0, gamma = 0;
+};
+
+// ThreeLevel.h:23-48: deck ThreeLevel.cpp:37-84 (distribution, count, i and j
+// ranges, lambda_a, lambda_b, gamma_a, gamma_b, t20, t21, t10, N_0, N_1); the
+// sites are the cells of ID 5 (the reference's "cells" placement).  The
+// default uses the Lorentz-oscillator coefficients; CPSFDTD_THREE_LITERAL=1
+// takes the reference's as written (its polarisation diverges).
+class ThreeLevel {
+public:
+    ThreeLevel(Structure &sS, const char *fileName)
+    {
+        cpsfdtd_detail::LineReader r(fileName);
+        cps_three_params p{};
+        r.line(0) >> distri;
+        r.line(1) >> NumSources;
+        r.line(2) >> i1 >> i2;
+        r.line(3) >> j1 >> j2;
+        r.line(4) >> p.lambda_a;
+        r.line(5) >> p.lambda_b;
+        r.line(6) >> p.gamma_a;
+        r.line(7) >> p.gamma_b;
+        r.line(8) >> p.t20;
+        r.line(9) >> p.t21;
+        r.line(10) >> p.t10;
+        r.line(11) >> p.N_0;
+        r.line(12) >> p.N_1;
+        p.gain_id = 5;
+        const char *lit = getenv("CPSFDTD_THREE_LITERAL");
+        p.literal = lit && lit[0] == '1';
+        lambda_a = p.lambda_a; lambda_b = p.lambda_b; gamma_a = p.gamma_a; gamma_b = p.gamma_b;
+        t20 = p.t20; t21 = p.t21; t10 = p.t10; N_0 = p.N_0; N_1 = p.N_1;
+        omega_a = 2.0 * 3.1415926535897932384626433832795 * 2.99792458E8 / lambda_a;  // ThreeLevel.cpp:96
+        omega_b = 2.0 * 3.1415926535897932384626433832795 * 2.99792458E8 / lambda_b;
+        g_ = sS.grid();
+        cpsfdtd_detail::check(cps_three_init(g_, &p), "ThreeLevel");
+    }
+    void UpdatePolarizationDensities(Field &fF)
+    {
+        cpsfdtd_detail::check(cps_op_three_polarization(fF.grid()), "UpdatePolarizationDensities");
+    }
+    void UpdateElectricField(Field &fF) { cpsfdtd_detail::check(cps_op_three_efield(fF.grid()), "UpdateElectricField"); }
+    void UpdateStatesPopulations(Field &fF)
+    {
+        cpsfdtd_detail::check(cps_op_three_populations(fF.grid()), "UpdateStatesPopulations");
+    }
+    // N0 N1 N2 per site (cells in (i,j,k) order): the reference's N0/N1/N2 arrays
+    std::vector<double> populations() const
+    {
+        int64_t n = 0;
+        cpsfdtd_detail::check(cps_three_populations(g_, nullptr, &n), "populations");
+        std::vector<double> out((size_t)n * 3);
+        cpsfdtd_detail::check(cps_three_populations(g_, out.data(), &n), "populations");
+        return out;
+    }
+
+    std::string distri;
+    int NumSources = 0, i1 = 0, i2 = 0, j1 = 0, j2 = 0;
+    double N_0 = 0, N_1 = 0;
+    double gamma_a = 0, gamma_b = 0, lambda_a = 0, lambda_b = 0, omega_a = 0, omega_b = 0;
+    double t20 = 0, t21 = 0, t10 = 0;
+
+private:
+    cps_grid *g_ = nullptr;
 };
 
 // FourLevelLaser.h:8-52: deck FourLevelLaser.cpp:37-93; gain sites are the

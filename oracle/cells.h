@@ -1,5 +1,5 @@
 /*
- * cells.h -- per-cell Drude-Lorentz and four-level-gain recursions of the
+ * cells.h -- per-cell Drude-Lorentz, four-level and three-level gain recursions of the
  * oracle restatement, shared by oracle.c and the reference harness (which
  * needs them because the reference has no 3-D Drude-Lorentz or gain class).
  *
@@ -212,6 +212,132 @@ static inline void gain_site_n(const gain_t *G, double *st, const double *E, int
     N[2] = G->t32t21dt / (G->t32t21_2 + G->t21dt * N[3] + G->t32dt * (1 - N[1])) *
            (N[2] * ((N[1] - 1) / G->t21 - N[3] / G->t32 + G->dt_2) + N[3] / G->t32_2 + s2 / G->homega_adt);
     N[0] = 2.0 - N[1] - N[2] - N[3];
+}
+
+/* ------------------------------------------------ three-level gain --- */
+
+#ifndef K_QE
+#define K_QE (-1.602176565E-19) /* electron charge, Constants.h:26 */
+#define K_ME 9.10938215E-31     /* electron mass, Constants.h:25 */
+#endif
+
+typedef struct {
+    int on;
+    int gain_id;
+    double CPa1, CPa2, CPa3, CPb1, CPb2, CPb3, CEP;
+    double CN2N2, CN2E, CN1N1, CN1N2, CN1E, CN0N2, CN0N1, CN0Ea, CN0Eb, CN0Ebx;
+    double N_0;
+    int64_t ncell;
+    int64_t *cell;
+    /* per site: Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3], E1[3], N0 N1 N2 N1_1 N2_1 */
+    double *state;
+} three_t;
+
+#define THREE_WORDS 26
+#define TS_PA 0
+#define TS_PA1 3
+#define TS_PA2 6
+#define TS_PB 9
+#define TS_PB1 12
+#define TS_PB2 15
+#define TS_E1 18
+#define TS_N0 21
+#define TS_N1 22
+#define TS_N2 23
+#define TS_N1_1 24
+#define TS_N2_1 25
+
+/* Coefficients: ThreeLevel.cpp:96-119 and :208.  literal = 1 takes them as
+ * the reference writes them: its oscillator coefficients CPa1 = 2/((dt^2 +
+ * w^2)(1/dt^2 + g/2dt)) and CPa2 = (2/dt^2 + 1/2dt)/(...) make P double every
+ * two steps, and the N0 update applies CN0Ea to the Pbx term.  literal = 0
+ * uses the Lorentz-oscillator discretisation (2/dt^2 - w^2)/(1/dt^2 + g/2dt)
+ * and (g/2dt - 1/dt^2)/(1/dt^2 + g/2dt), and CN0Eb on every b term. */
+static void three_coeffs(three_t *T3, double dt, double lambda_a, double lambda_b, double gamma_a,
+                         double gamma_b, double t20, double t21, double t10, double N_0, int literal)
+{
+    const double omega_a = 2.0 * K_PI * K_C / lambda_a;
+    const double omega_b = 2.0 * K_PI * K_C / lambda_b;
+    if (literal) {
+        T3->CPa1 = 2 / ((dt * dt + omega_a * omega_a) * (1 / (dt * dt) + gamma_a / (2 * dt)));
+        T3->CPa2 = (2 / (dt * dt) + 1 / (2 * dt)) / (1 / (dt * dt) + gamma_a / (2 * dt));
+        T3->CPb1 = 2 / ((dt * dt + omega_b * omega_b) * (1 / (dt * dt) + gamma_b / (2 * dt)));
+        T3->CPb2 = (2 / (dt * dt) + 1 / (2 * dt)) / (1 / (dt * dt) + gamma_b / (2 * dt));
+    } else {
+        T3->CPa1 = (2 / (dt * dt) - omega_a * omega_a) / (1 / (dt * dt) + gamma_a / (2 * dt));
+        T3->CPa2 = (gamma_a / (2 * dt) - 1 / (dt * dt)) / (1 / (dt * dt) + gamma_a / (2 * dt));
+        T3->CPb1 = (2 / (dt * dt) - omega_b * omega_b) / (1 / (dt * dt) + gamma_b / (2 * dt));
+        T3->CPb2 = (gamma_b / (2 * dt) - 1 / (dt * dt)) / (1 / (dt * dt) + gamma_b / (2 * dt));
+    }
+    T3->CPa3 = (K_QE * K_QE / K_ME) / (1 / (dt * dt) + gamma_a / (2 * dt)) / N_0;
+    T3->CPb3 = (K_QE * K_QE / K_ME) / (1 / (dt * dt) + gamma_b / (2 * dt)) / N_0;
+    T3->CN2N2 = (1.0 / dt - 1.0 / (2.0 * t20) - 1.0 / (2.0 * t21)) / (1.0 / dt + 1.0 / (2.0 * t20) + 1.0 / (2.0 * t21));
+    T3->CN2E = (1.0 / (2.0 * dt * K_HPLANCK * omega_a / 2.0 / K_PI)) / (1.0 / dt + 1.0 / (2.0 * t20) + 1.0 / (2.0 * t21));
+    T3->CN1N1 = (1.0 / dt - 1.0 / (2.0 * t10)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    T3->CN1N2 = (1.0 / (2.0 * t21)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    T3->CN1E = (1.0 / (2.0 * dt * K_HPLANCK * omega_b / 2.0 / K_PI)) / (1.0 / dt + 1.0 / (2.0 * t10));
+    T3->CN0N1 = dt / (2.0 * t10);
+    T3->CN0N2 = dt / (2.0 * t20);
+    T3->CN0Ea = 1.0 / (2.0 * K_HPLANCK * omega_a / 2.0 / K_PI);
+    T3->CN0Eb = 1.0 / (2.0 * K_HPLANCK * omega_b / 2.0 / K_PI);
+    T3->CN0Ebx = literal ? T3->CN0Ea : T3->CN0Eb;
+    T3->CEP = 1.0 / dt / K_EPS0;
+    T3->N_0 = N_0;
+}
+
+/* ThreeLevel.cpp:200-206: P, E1, N1, N2 zero, N0 = N_0 */
+static void three_site_init(double *st, double N_0)
+{
+    memset(st, 0, sizeof(double) * THREE_WORDS);
+    st[TS_N0] = N_0;
+}
+
+/* UpdatePolarizationDensities at one site, ThreeLevel.cpp:216-245; nc = 2 (TE) or 3 */
+static inline void three_site_p(const three_t *T3, double *st, const double *E, int nc)
+{
+    const double N0 = st[TS_N0], N1 = st[TS_N1], N2 = st[TS_N2];
+    for (int c = 0; c < nc; ++c) {
+        st[TS_PA2 + c] = st[TS_PA1 + c];
+        st[TS_PA1 + c] = st[TS_PA + c];
+        st[TS_PA + c] = T3->CPa1 * st[TS_PA + c] + T3->CPa2 * st[TS_PA2 + c] + E[c] * T3->CPa3 * (N2 - N0);
+    }
+    for (int c = 0; c < nc; ++c) {
+        st[TS_PB2 + c] = st[TS_PB1 + c];
+        st[TS_PB1 + c] = st[TS_PB + c];
+        st[TS_PB + c] = T3->CPb1 * st[TS_PB + c] + T3->CPb2 * st[TS_PB2 + c] + E[c] * T3->CPb3 * (N1 - N0);
+    }
+    for (int c = 0; c < nc; ++c) st[TS_E1 + c] = E[c];
+}
+
+/* UpdateElectricField at one site, ThreeLevel.cpp:248-255 */
+static inline void three_site_e(const three_t *T3, const double *st, double *E, int nc)
+{
+    for (int c = 0; c < nc; ++c)
+        E[c] = E[c] - T3->CEP * (st[TS_PA + c] - st[TS_PA1 + c] + st[TS_PB + c] - st[TS_PB1 + c]);
+}
+
+/* UpdateStatesPopulations at one site, ThreeLevel.cpp:258-266 (the Ez terms,
+ * absent in the reference's 2-D class, follow the Ex and Ey forms) */
+static inline void three_site_n(const three_t *T3, double *st, const double *E, int nc)
+{
+    const double *Pa = st + TS_PA, *Pa1 = st + TS_PA1, *Pb = st + TS_PB, *Pb1 = st + TS_PB1;
+    const double *E1 = st + TS_E1;
+    st[TS_N2_1] = st[TS_N2];
+    double n2 = T3->CN2N2 * st[TS_N2] + T3->CN2E * (E[0] + E1[0]) * (Pa[0] - Pa1[0]) +
+                T3->CN2E * (E[1] + E1[1]) * (Pa[1] - Pa1[1]);
+    if (nc == 3) n2 = n2 + T3->CN2E * (E[2] + E1[2]) * (Pa[2] - Pa1[2]);
+    st[TS_N2] = n2;
+    st[TS_N1_1] = st[TS_N1];
+    double n1 = T3->CN1N1 * st[TS_N1] + T3->CN1N2 * (st[TS_N2] + st[TS_N2_1]) +
+                T3->CN1E * (E[0] + E1[0]) * (Pb[0] - Pb1[0]) + T3->CN1E * (E[1] + E1[1]) * (Pb[1] - Pb1[1]);
+    if (nc == 3) n1 = n1 + T3->CN1E * (E[2] + E1[2]) * (Pb[2] - Pb1[2]);
+    st[TS_N1] = n1;
+    double n0 = st[TS_N0] + T3->CN0N2 * (st[TS_N2] + st[TS_N2_1]) + T3->CN0N1 * (st[TS_N1] + st[TS_N1_1]) -
+                T3->CN0Ea * (E[0] + E1[0]) * (Pa[0] - Pa1[0]) - T3->CN0Ea * (E[1] + E1[1]) * (Pa[1] - Pa1[1]) -
+                T3->CN0Ebx * (E[0] + E1[0]) * (Pb[0] - Pb1[0]) - T3->CN0Eb * (E[1] + E1[1]) * (Pb[1] - Pb1[1]);
+    if (nc == 3)
+        n0 = n0 - T3->CN0Ea * (E[2] + E1[2]) * (Pa[2] - Pa1[2]) - T3->CN0Eb * (E[2] + E1[2]) * (Pb[2] - Pb1[2]);
+    st[TS_N0] = n0;
 }
 
 #endif

@@ -85,6 +85,7 @@ struct orc {
     pml_t pml;
     dl_t dl;
     gain_t gain;
+    three_t three;
     tfsf_t tfsf;
     int nsrc;
     src_t *src;
@@ -152,6 +153,7 @@ void orc_destroy(orc *o)
     }
     free(o->dl.cell); free(o->dl.state);
     free(o->gain.cell); free(o->gain.state);
+    free(o->three.cell); free(o->three.state);
     free(o->tfsf.einc); free(o->tfsf.hinc);
     for (int s = 0; s < o->nsrc; ++s) free(o->src[s].wave);
     free(o->src);
@@ -636,9 +638,88 @@ int orc_gain_populations(const orc *o, double *out)
     return 0;
 }
 
+/* ------------------------------------------------- three-level gain --- */
+
+/* ThreeLevel::ThreeLevel (ThreeLevel.cpp:29-209) with the "cells" placement:
+ * the E-range cells of ID gain_id (the reference's extra site past the list,
+ * :147-149, sits at (Nx, Ny) where E stays zero, and is left out) */
+int orc_three_init(orc *o, int gain_id, double lambda_a, double lambda_b, double gamma_a, double gamma_b,
+                   double t20, double t21, double t10, double N_0, int literal)
+{
+    three_t *T3 = &o->three;
+    if (gain_id < 0 || gain_id > 255 || gain_id == ID_DISPERSIVE || gain_id == ID_PEC || o->gain.on) return 1;
+    T3->gain_id = gain_id;
+    three_coeffs(T3, o->dt, lambda_a, lambda_b, gamma_a, gamma_b, t20, t21, t10, N_0, literal);
+    int64_t n = 0;
+    for (int i = 1; i < o->nx; ++i)
+        for (int j = 1; j < o->ny; ++j)
+            for (int k = 1; k < o->nz; ++k)
+                if (o->id[IDX(o, i, j, k)] == gain_id) ++n;
+    T3->ncell = n;
+    T3->cell = (int64_t *)zalloc(sizeof(int64_t) * n);
+    T3->state = (double *)zalloc(sizeof(double) * n * THREE_WORDS);
+    n = 0;
+    for (int i = 1; i < o->nx; ++i)
+        for (int j = 1; j < o->ny; ++j)
+            for (int k = 1; k < o->nz; ++k)
+                if (o->id[IDX(o, i, j, k)] == gain_id) {
+                    three_site_init(T3->state + n * THREE_WORDS, N_0);
+                    T3->cell[n++] = IDX(o, i, j, k);
+                }
+    T3->on = 1;
+    return 0;
+}
+
+void orc_op_three_p(orc *o)
+{
+    three_t *T3 = &o->three;
+    if (!T3->on) return;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < T3->ncell; ++c) {
+        const int64_t g = T3->cell[c];
+        const double E[3] = {o->F[EX][g], o->F[EY][g], o->F[EZ][g]};
+        three_site_p(T3, T3->state + c * THREE_WORDS, E, 3);
+    }
+}
+
+void orc_op_three_e(orc *o)
+{
+    three_t *T3 = &o->three;
+    if (!T3->on) return;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < T3->ncell; ++c) {
+        const int64_t g = T3->cell[c];
+        double E[3] = {o->F[EX][g], o->F[EY][g], o->F[EZ][g]};
+        three_site_e(T3, T3->state + c * THREE_WORDS, E, 3);
+        o->F[EX][g] = E[0]; o->F[EY][g] = E[1]; o->F[EZ][g] = E[2];
+    }
+}
+
+void orc_op_three_n(orc *o)
+{
+    three_t *T3 = &o->three;
+    if (!T3->on) return;
+#pragma omp parallel for schedule(static)
+    for (int64_t c = 0; c < T3->ncell; ++c) {
+        const int64_t g = T3->cell[c];
+        const double E[3] = {o->F[EX][g], o->F[EY][g], o->F[EZ][g]};
+        three_site_n(T3, T3->state + c * THREE_WORDS, E, 3);
+    }
+}
+
+/* N0 N1 N2 per site, sites in [i][j][k] order */
+int orc_three_populations(const orc *o, double *out)
+{
+    const three_t *T3 = &o->three;
+    if (!T3->on) return 1;
+    for (int64_t c = 0; c < T3->ncell; ++c)
+        for (int q = 0; q < 3; ++q) out[c * 3 + q] = T3->state[c * THREE_WORDS + TS_N0 + q];
+    return 0;
+}
+
 int64_t orc_count_cells(const orc *o, int which)
 {
-    return which == 0 ? o->dl.ncell : o->gain.ncell;
+    return which == 0 ? o->dl.ncell : which == 1 ? o->gain.ncell : o->three.ncell;
 }
 
 /* ------------------------------------------------------------- TF/SF --- */
@@ -978,6 +1059,9 @@ void orc_step(orc *o, int nsteps)
         orc_op_gain_p(o);
         orc_op_gain_e(o);
         orc_op_gain_n(o);
+        orc_op_three_p(o);
+        orc_op_three_e(o);
+        orc_op_three_n(o);
         orc_op_tfsf_e(o, n);
         orc_op_sources(o, n);
         orc_op_e_pml(o);
@@ -1044,10 +1128,24 @@ int orc2d_run(int nx, int ny, double dx, double dy, double dt, const uint8_t *id
         dls = (double *)zalloc(sizeof(double) * n2 * 2 * D.stride);
     }
     gain_t G; memset(&G, 0, sizeof(G));
+    three_t T3; memset(&T3, 0, sizeof(T3));
     int64_t ng = 0;
     int64_t *gcell = NULL;
     double *gst = NULL;
-    if (use_gain) {
+    const int words = use_gain == 2 ? THREE_WORDS : GAIN_WORDS;
+    if (use_gain == 2) {
+        /* gp: lambda_a lambda_b gamma_a gamma_b t20 t21 t10 N_0 literal */
+        three_coeffs(&T3, dt, gp[0], gp[1], gp[2], gp[3], gp[4], gp[5], gp[6], gp[7], (int)gp[8]);
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+                if (ids2d[I2(i, j)] == 5) ++ng;
+        gcell = (int64_t *)zalloc(sizeof(int64_t) * (ng + 1));
+        gst = (double *)zalloc(sizeof(double) * (ng + 1) * THREE_WORDS);
+        ng = 0;
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+                if (ids2d[I2(i, j)] == 5) { three_site_init(gst + ng * THREE_WORDS, gp[7]); gcell[ng++] = I2(i, j); }
+    } else if (use_gain) {
         gain_coeffs(&G, dt, dx, dy, gp[0], gp[1], gp[2], gp[3], gp[4], gp[5], gp[6], gp[7], gp[8], gp[9]);
         for (int i = 0; i < nx; ++i)
             for (int j = 0; j < ny; ++j)
@@ -1087,7 +1185,21 @@ int orc2d_run(int nx, int ny, double dx, double dy, double dt, const uint8_t *id
             for (int j = 1; j < ny; ++j) Ex[I2(0, j)] = aE[0] * Ex[I2(0, j)] + bE[0] * (Hz[I2(0, j)] - Hz[I2(0, j - 1)]) * cy;
             for (int i = 1; i < nx; ++i) Ey[I2(i, 0)] = aE[0] * Ey[I2(i, 0)] - bE[0] * (Hz[I2(i, 0)] - Hz[I2(i - 1, 0)]) * cx;
         }
-        if (use_gain) {
+        if (use_gain == 2) {
+            for (int64_t c = 0; c < ng; ++c) {
+                double E[3] = {Ex[gcell[c]], Ey[gcell[c]], 0.0};
+                three_site_p(&T3, gst + c * words, E, 2);
+            }
+            for (int64_t c = 0; c < ng; ++c) {
+                double E[3] = {Ex[gcell[c]], Ey[gcell[c]], 0.0};
+                three_site_e(&T3, gst + c * words, E, 2);
+                Ex[gcell[c]] = E[0]; Ey[gcell[c]] = E[1];
+            }
+            for (int64_t c = 0; c < ng; ++c) {
+                double E[3] = {Ex[gcell[c]], Ey[gcell[c]], 0.0};
+                three_site_n(&T3, gst + c * words, E, 2);
+            }
+        } else if (use_gain) {
             for (int64_t c = 0; c < ng; ++c) {
                 double E[3] = {Ex[gcell[c]], Ey[gcell[c]], 0.0};
                 gain_site_p(&G, gst + c * GAIN_WORDS, E, 2);

@@ -99,7 +99,15 @@ int orc_port_read(const orc *o, int port, double *out);      /* [npts][6] */
 int orc_port_dft_read(const orc *o, int port, double *out);  /* [npts][ncomp][nfreq][2] */
 int orc_tfsf_tables(const orc *o, double *einc, double *hinc); /* Nt+1 each */
 int orc_gain_populations(const orc *o, double *out);          /* [ncells][4] N0..N3 */
-int64_t orc_count_cells(const orc *o, int which);             /* 0: DL cells, 1: gain cells */
+/* three-level gain (ThreeLevel.cpp), "cells" placement on ID gain_id; literal
+ * as three_coeffs in cells.h (1: the reference's coefficients as written) */
+int orc_three_init(orc *o, int gain_id, double lambda_a, double lambda_b, double gamma_a, double gamma_b,
+                   double t20, double t21, double t10, double N_0, int literal);
+void orc_op_three_p(orc *o);
+void orc_op_three_e(orc *o);
+void orc_op_three_n(orc *o);
+int orc_three_populations(const orc *o, double *out);
+int64_t orc_count_cells(const orc *o, int which); /* 0: DL cells, 1: four-level, 2: three-level gain cells */
 
 /* 2-D TE drivers used to pin the recursions against the reference's 2-D
  * classes.  ids2d is [nx+1][ny+1] (j fastest); the source adds wave[n] to Hz
@@ -110,7 +118,9 @@ int orc2d_run(int nx, int ny, double dx, double dy, double dt,
               int use_dl, double dl_sigma, double dl_epsInf, int nD, const double *fD,
               const double *gD, int nL, const double *fL, const double *dL,
               const double *depsL, int dl_literal,
-              int use_gain, const double *gain_params /* 10: la lb ga gb t30 t32 t21 t10 N_0 pump */,
+              int use_gain /* 1: four-level, 2: three-level */,
+              const double *gain_params /* four-level: la lb ga gb t30 t32 t21 t10 N_0 pump;
+                                           three-level: la lb ga gb t20 t21 t10 N_0 literal */,
               int si, int sj, const double *wave, int nsteps,
               double *Ex, double *Ey, double *Hz);
 

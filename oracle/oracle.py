@@ -65,10 +65,13 @@ def lib():
         L.orc_port_read.argtypes = [P, C.c_int, dp]
         L.orc_port_dft_read.argtypes = [P, C.c_int, dp]
         L.orc_gain_populations.argtypes = [P, dp]
+        L.orc_three_init.argtypes = [P, C.c_int] + [C.c_double] * 8 + [C.c_int]
+        L.orc_three_populations.argtypes = [P, dp]
         L.orc_count_cells.restype = C.c_int64
         L.orc_count_cells.argtypes = [P, C.c_int]
         for name in ("orc_op_h_bulk", "orc_op_h_pml", "orc_op_e_bulk", "orc_op_e_pml", "orc_op_dl",
-                     "orc_op_gain_p", "orc_op_gain_e", "orc_op_gain_n"):
+                     "orc_op_gain_p", "orc_op_gain_e", "orc_op_gain_n",
+                     "orc_op_three_p", "orc_op_three_e", "orc_op_three_n"):
             getattr(L, name).argtypes = [P]
         for name in ("orc_op_tfsf_h", "orc_op_tfsf_e", "orc_op_sources", "orc_op_ports"):
             getattr(L, name).argtypes = [P, C.c_int]
@@ -126,6 +129,11 @@ class Oracle:
             g = dk.gain
             assert o.L.orc_gain_init(o.h, 5, g["lambda_a"], g["lambda_b"], g["gamma_a"], g["gamma_b"],
                                      g["t30"], g["t32"], g["t21"], g["t10"], g["N_0"], g.get("pump", 0.0)) == 0
+        if getattr(dk, "three", None):
+            t3 = dk.three
+            assert o.L.orc_three_init(o.h, int(t3.get("gain_id", 5)), t3["lambda_a"], t3["lambda_b"], t3["gamma_a"],
+                                      t3["gamma_b"], t3["t20"], t3["t21"], t3["t10"], t3["N_0"],
+                                      int(t3.get("literal", 0))) == 0
         if dk.tfsf:
             t = dk.tfsf_abi()
             tp = TfsfParams(t["lambda_"], t["dlambda"], t["w0"], t["z0"], t["i0"], t["j0"], t["k0"],
@@ -191,6 +199,13 @@ class Oracle:
         n = self.L.orc_count_cells(self.h, 1)
         out = np.empty((n, 4))
         self.L.orc_gain_populations(self.h, out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
+    def three_populations(self):
+        """N0 N1 N2 per three-level site, sites in [i][j][k] order"""
+        n = self.L.orc_count_cells(self.h, 2)
+        out = np.empty((n, 3))
+        self.L.orc_three_populations(self.h, out.ctypes.data_as(C.POINTER(C.c_double)))
         return out
 
 
@@ -264,7 +279,16 @@ def ref_bench(dk, warm, timed, threads=0, exe=None, timeout=900):
         shutil.rmtree(workdir, ignore_errors=True)
 
 
-def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, timeout=120):
+def write_three_deck(path, three):
+    """ThreeLevel.txt in the reference's format (ThreeLevel.cpp:37-84), "cells" placement."""
+    with open(path, "w") as f:
+        f.write("cells\n0\n0 0\n0 0\n")
+        for key in ("lambda_a", "lambda_b", "gamma_a", "gamma_b", "t20", "t21", "t10", "N_0"):
+            f.write(f"{float(three[key])!r}\n")
+        f.write("0\n")
+
+
+def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, three=None, timeout=120):
     """Run the reference's 2-D Drude_Lorentz / FourLevelLaser / Drude classes.
     params: dict nx ny dx dy dt nsteps si sj; drude: dict epsInf fP sigma gamma
     (Hz) for the single-pole Drude class.  Returns (Ex, Ey, Hz)."""
@@ -273,7 +297,8 @@ def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, timeou
         p = params
         with open(os.path.join(workdir, "params2d.txt"), "w") as f:
             f.write(f"{p['nx']} {p['ny']} {float(p['dx'])!r} {float(p['dy'])!r} {float(p['dt'])!r} {p['nsteps']} {p['si']} {p['sj']} "
-                    f"{1 if dl else 0} {1 if gain else 0} {int((dl or {}).get('literal', 0))} {1 if drude else 0}\n")
+                    f"{1 if dl else 0} {1 if gain else 0} {int((dl or {}).get('literal', 0))} {1 if drude else 0} "
+                    f"{1 if three else 0}\n")
         with open(os.path.join(workdir, "media2d.txt"), "w") as f:
             f.write(f"{len(media)}\n")
             for m in media:
@@ -287,6 +312,8 @@ def run_ref2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, timeou
                     f.write(f"{float(a)!r}\t{float(b)!r}\n")
                 for a, b, c in zip(dl["fL"], dl["dL"], dl["depsL"]):
                     f.write(f"{float(a)!r}\t{float(b)!r}\t{float(c)!r}\n")
+        if three:
+            write_three_deck(os.path.join(workdir, "ThreeLevel.txt"), three)
         if drude:
             with open(os.path.join(workdir, "Drude.txt"), "w") as f:
                 for key in ("epsInf", "fP", "sigma", "gamma"):
@@ -315,8 +342,9 @@ def drude_as_dl(drude):
                 fL=[], dL=[], depsL=[], literal=2)
 
 
-def run_orc2d(params, media, ids2d, wave, dl=None, gain=None, drude=None):
-    """The oracle's 2-D TE driver on the same problem as run_ref2d."""
+def run_orc2d(params, media, ids2d, wave, dl=None, gain=None, drude=None, three=None):
+    """The oracle's 2-D TE driver on the same problem as run_ref2d; three: the
+    three-level gain with literal = 1 reproducing the reference's class."""
     L = lib()
     if drude:
         dl = drude_as_dl(drude)
@@ -329,14 +357,18 @@ def run_orc2d(params, media, ids2d, wave, dl=None, gain=None, drude=None):
     empty = _dp(np.zeros(1))
     d = dl or dict(sigma=0.0, epsInf=1.0, fD=[], gD=[], fL=[], dL=[], depsL=[])
     arrs = [_dp(np.array(d[k] if len(d[k]) else [0.0], dtype=np.float64)) for k in ("fD", "gD", "fL", "dL", "depsL")]
-    gp = _dp(np.array([gain[k] for k in ("lambda_a", "lambda_b", "gamma_a", "gamma_b", "t30", "t32", "t21", "t10", "N_0")]
-                      + [gain.get("pump", 0.0)]) if gain else np.zeros(10))
+    if three:
+        gp = _dp(np.array([three[k] for k in ("lambda_a", "lambda_b", "gamma_a", "gamma_b", "t20", "t21", "t10", "N_0")]
+                          + [float(three.get("literal", 0)), 0.0]))
+    else:
+        gp = _dp(np.array([gain[k] for k in ("lambda_a", "lambda_b", "gamma_a", "gamma_b", "t30", "t32", "t21", "t10",
+                                             "N_0")] + [gain.get("pump", 0.0)]) if gain else np.zeros(10))
     w = _dp(wave)
     rc = L.orc2d_run(p["nx"], p["ny"], p["dx"], p["dy"], p["dt"], ids2d.ctypes.data, len(m),
                      cols[0][1], cols[1][1], cols[2][1], cols[3][1],
                      1 if dl else 0, d["sigma"], d["epsInf"], len(d["fD"]), arrs[0][1], arrs[1][1],
                      len(d["fL"]), arrs[2][1], arrs[3][1], arrs[4][1], int(d.get("literal", 0)),
-                     1 if gain else 0, gp[1], p["si"], p["sj"], w[1], p["nsteps"],
+                     2 if three else (1 if gain else 0), gp[1], p["si"], p["sj"], w[1], p["nsteps"],
                      Ex.ctypes.data_as(C.POINTER(C.c_double)), Ey.ctypes.data_as(C.POINTER(C.c_double)),
                      Hz.ctypes.data_as(C.POINTER(C.c_double)))
     del empty

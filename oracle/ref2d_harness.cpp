@@ -8,7 +8,7 @@
 // TEST INFRASTRUCTURE ONLY.
 //
 // Usage: ref2d_harness <deck_dir> <out_dir>
-//   params2d.txt : nx ny dx dy dt nsteps si sj use_dl use_gain [dl_literal [use_drude]]
+//   params2d.txt : nx ny dx dy dt nsteps si sj use_dl use_gain [dl_literal [use_drude [use_three]]]
 //   With dl_literal 0 the constructed Drude_Lorentz gets C1 and C5 overwritten
 //   with the values the ADE discretisation gives (Drude_Lorentz.cpp:96 has the
 //   wrong sign on sigma*dt + dt*sum(beta), :106 lacks a factor dt); the update
@@ -17,7 +17,8 @@
 //   ids2d.bin    : uint8 [nx+1][ny+1], j fastest
 //   wave.bin     : nsteps doubles, added to Hz[si][sj] after each H update
 //   DrudeLorentz.txt / FourLevelLaser.txt / Drude.txt : reference-format decks;
-//   use_drude runs the single-pole Drude class (Drude.cpp) as the E update
+//   use_drude runs the single-pole Drude class (Drude.cpp) as the E update;
+//   use_three runs the three-level gain class (ThreeLevel.cpp, deck ThreeLevel.txt)
 #include "stdafx.h"
 #include "Constants.h"
 #include "Structure.h"
@@ -39,6 +40,7 @@
 #undef private
 #include "FourLevelLaser.h"
 #include "Drude.h"
+#include "ThreeLevel.h"
 
 void *operator new(std::size_t n) { void *p = calloc(n ? n : 1, 1); if (!p) throw std::bad_alloc(); return p; }
 void *operator new[](std::size_t n) { void *p = calloc(n ? n : 1, 1); if (!p) throw std::bad_alloc(); return p; }
@@ -60,13 +62,14 @@ int main(int argc, char **argv)
 {
     if (argc < 3) die("usage");
     const std::string dir = std::string(argv[1]) + "/", out = std::string(argv[2]) + "/";
-    int nx, ny, nsteps, si, sj, use_dl, use_gain, dl_literal = 1, use_drude = 0;
+    int nx, ny, nsteps, si, sj, use_dl, use_gain, dl_literal = 1, use_drude = 0, use_three = 0;
     double dx, dy, dt;
     {
         std::ifstream p(dir + "params2d.txt");
         if (!(p >> nx >> ny >> dx >> dy >> dt >> nsteps >> si >> sj >> use_dl >> use_gain)) die("params");
         if (!(p >> dl_literal)) dl_literal = 1;
         if (!(p >> use_drude)) use_drude = 0;
+        if (!(p >> use_three)) use_three = 0;
     }
     int nm;
     std::ifstream mi(dir + "media2d.txt");
@@ -111,6 +114,10 @@ int main(int argc, char **argv)
     std::vector<char> dln(dlf.begin(), dlf.end()), gln(glf.begin(), glf.end()), drn(drf.begin(), drf.end());
     dln.push_back(0); gln.push_back(0); drn.push_back(0);
     Drude *DR = use_drude ? new Drude(S, drn.data()) : nullptr;
+    std::string tlf = dir + "ThreeLevel.txt";
+    std::vector<char> tln(tlf.begin(), tlf.end());
+    tln.push_back(0);
+    ThreeLevel *TL = use_three ? new ThreeLevel(S, tln.data()) : nullptr;
     Drude_Lorentz *DL = use_dl ? new Drude_Lorentz(S, dln.data()) : nullptr;
     FourLevelLaser *FL = use_gain ? new FourLevelLaser(S, gln.data()) : nullptr;
     if (DL && !dl_literal) {
@@ -144,6 +151,11 @@ int main(int argc, char **argv)
             FL->UpdatePolarizationDensities(F);
             FL->UpdateElectricField(F);
             FL->UpdateStatesPopulations(F);
+        }
+        if (TL) {
+            TL->UpdatePolarizationDensities(F);
+            TL->UpdateElectricField(F);
+            TL->UpdateStatesPopulations(F);
         }
     }
     std::vector<double> buf((size_t)(nx + 1) * (ny + 1));

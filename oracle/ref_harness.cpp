@@ -170,6 +170,7 @@ int main(int argc, char **argv)
             else if (key == "dl") { s >> dl_file; if (!(s >> dl_literal)) dl_literal = 0; }
             else if (key == "gain") s >> gain_file;
             else if (key == "drude") s >> drude_file;
+            else if (key == "three") die("the three-level gain runs in the oracle and the engine only (its reference class is 2-D)");
             else if (key == "record_ports") s >> record_ports;
             else if (key == "bench") s >> warm >> timed;
             else if (key == "threads") s >> threads;

@@ -44,6 +44,8 @@ int main(int argc, char **argv)
         if (exists(dir + "/Drude.txt")) DR.reset(new Drude(S, (dir + "/Drude.txt").c_str()));
         std::unique_ptr<FourLevelLaser> FL;
         if (exists(dir + "/FourLevelLaser.txt")) FL.reset(new FourLevelLaser(S, (dir + "/FourLevelLaser.txt").c_str()));
+        std::unique_ptr<ThreeLevel> TL;
+        if (exists(dir + "/ThreeLevel.txt")) TL.reset(new ThreeLevel(S, (dir + "/ThreeLevel.txt").c_str()));
         std::unique_ptr<TF_SF> tfsf;
         if (exists(dir + "/TF_SF.txt")) tfsf.reset(new TF_SF(S, (dir + "/TF_SF.txt").c_str()));
         std::vector<std::unique_ptr<PlainPort>> ports;
@@ -65,6 +67,11 @@ int main(int argc, char **argv)
                 FL->UpdatePolarizationDensities(F);
                 FL->UpdateElectricField(F);
                 FL->UpdateStatesPopulations(F);
+            }
+            if (TL) {
+                TL->UpdatePolarizationDensities(F);
+                TL->UpdateElectricField(F);
+                TL->UpdateStatesPopulations(F);
             }
             if (tfsf) tfsf->UpdateEField(n, F, S);
             if (pml) pml->UpdateCPMLEFields(F);

@@ -61,6 +61,13 @@ def _grid2d(kind):
     ids = np.zeros((nx + 1, ny + 1), np.uint8)
     p = dict(nx=nx, ny=ny, dx=d, dy=d, dt=dt, nsteps=240, si=10, sj=24)
     wave = decks.gaussian_sine(240, dt, 550e-9, 4e-15, 12e-15)
+    if kind == "three_literal":
+        # the reference's ThreeLevel class as written: its polarisation doubles
+        # every two steps, so the case stops after 60 steps, before it blows up
+        ids[16:34, 14:36] = 5
+        media = [(1, 1, 0, 0)] * 5 + [(2.25, 1, 0, 0)]
+        p = dict(p, nsteps=60)
+        return p, media, ids, 1e3 * wave[:60], {"three": decks.three_params_laser(literal=1)}
     if kind == "gain":
         ids[16:34, 14:36] = 5
         media = [(1, 1, 0, 0)] * 5 + [(2.25, 1, 0, 0)]
@@ -77,4 +84,5 @@ def _grid2d(kind):
 
 
 CASES_2D = {"dl": lambda: _grid2d("dl"), "dl_literal": lambda: _grid2d("dl_literal"),
-            "gain": lambda: _grid2d("gain"), "drude": lambda: _grid2d("drude")}
+            "gain": lambda: _grid2d("gain"), "drude": lambda: _grid2d("drude"),
+            "three_literal": lambda: _grid2d("three_literal")}

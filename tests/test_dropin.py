@@ -35,7 +35,7 @@ def test_dropin_main_builds_and_fails_loudly(tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("record", ["1", "0"])
-@pytest.mark.parametrize("case", ["dispersive", "dielectric", "drude"])
+@pytest.mark.parametrize("case", ["dispersive", "dielectric", "drude", "three"])
 def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
     """record "1": the classes' calls run as fused steps (the default);
     "0": routine by routine."""
@@ -46,6 +46,12 @@ def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
     elif case == "drude":  # the single-pole Drude class (Drude.txt deck)
         dk = decks.config2(n=32, steps=40, nfreq=2)
         dk.dl = decks.drude_as_dl(decks.drude_params_metal())
+    elif case == "three":  # the three-level gain class (ThreeLevel.txt deck) under a TF/SF beam
+        dk = decks.config3(n=32, steps=40, nfreq=0, port=False)
+        dk.gain = None
+        dk.three = decks.three_params_laser()
+        dk.sources = []
+        dk.tfsf = decks.config2(n=32, steps=40, nfreq=1).tfsf
     else:
         dk = decks.config1(n=28, steps=40)
         dk.sources = []  # point sources are main.cpp code, not a class: drive it with a TF/SF beam instead
@@ -71,6 +77,10 @@ def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
         L.orc_op_e_bulk(o.h)
         if dk.dl:
             L.orc_op_dl(o.h)
+        if dk.three:
+            L.orc_op_three_p(o.h)
+            L.orc_op_three_e(o.h)
+            L.orc_op_three_n(o.h)
         L.orc_op_tfsf_e(o.h, n)
         L.orc_op_e_pml(o.h)
         L.orc_op_ports(o.h, n)

@@ -34,8 +34,18 @@ def _c2_drude():
     return dk
 
 
+def _c3_three():
+    """The laser deck with the three-level gain class (ThreeLevel.cpp, Lorentz
+    oscillators) on its gain cells instead of the four-level one."""
+    dk = decks.config3(n=40, steps=100, nfreq=4)
+    dk.gain = None
+    dk.three = decks.three_params_laser()
+    return dk
+
+
 CASES = {"c1": lambda: decks.config1(n=32, steps=120),
          "c2_drude": _c2_drude,
+         "c3_three": _c3_three,
          "c2": lambda: decks.config2(n=48, steps=100, nfreq=8),
          "c2_cw": gc.c2_cw,
          "c3": lambda: decks.config3(n=40, steps=100, nfreq=4),
@@ -152,3 +162,28 @@ def test_drude_entry_point_equals_dl_form():
     b.step(30, cps.FUSED)
     for c in range(6):
         assert np.array_equal(a.field(c), b.field(c))
+
+
+def test_three_level_populations_match_oracle(oracle_runs):
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs["c3_three"]
+    want = o.three_populations()
+    assert want.shape[0] > 0 and np.abs(want[:, 1:]).max() > 0  # the field moved population
+    for prec, tol, path in ((cps.FP64, 1e-12, cps.FUSED), (cps.FP64, 1e-12, cps.PLAIN), (cps.FP32, 1e-6, cps.FUSED)):
+        g = cps.Grid.from_deck(dk, prec, ids=ids, port_points_list=pts)
+        g.step(dk.nsteps, path)
+        got = g.three_populations()
+        assert got.shape == want.shape
+        assert np.abs(got - want).max() <= tol * np.abs(want).max()
+
+
+def test_three_level_rejects_a_second_gain_and_batches():
+    import cpsfdtd_b200 as cps
+    dk = _c3_three()
+    g = cps.Grid.from_deck(dk, cps.FP32)
+    with pytest.raises(cps.CpsError):
+        g.gain_init(decks.gain_params_laser())
+    b = cps.Batch(cps.FP32)
+    with pytest.raises(cps.CpsError):
+        b.add(g)
+    b.close()

@@ -33,6 +33,10 @@ def _reference_calls(g, dk, n):
         g.op("gain_polarization")
         g.op("gain_efield")
         g.op("gain_populations")
+    if dk.three:
+        g.op("three_polarization")
+        g.op("three_efield")
+        g.op("three_populations")
     if dk.tfsf:
         g.op("tfsf_e", n, 0x3F)
     if dk.sources:
@@ -62,7 +66,15 @@ _DECKS = {
     "dispersive": lambda: decks.config2(n=40, steps=1, nfreq=3),
     "dielectric_sources": lambda: decks.config1(n=36, steps=1),
     "laser": lambda: decks.config4_member(40, 48, 36, seed=3, steps=1, nfreq=2),
+    "three_level": lambda: _three(),
 }
+
+
+def _three():
+    dk = decks.config4_member(40, 48, 36, seed=6, steps=1, nfreq=2)
+    dk.gain = None
+    dk.three = decks.three_params_laser()
+    return dk
 
 
 @pytest.mark.parametrize("name", sorted(_DECKS))

@@ -87,3 +87,24 @@ def test_drude_kat_is_dispersive_and_lossy(oracle_mod):
     literal_dl = dict(oracle_mod.drude_as_dl(kw["drude"]), literal=1)
     other = oracle_mod.run_orc2d(p, media, ids, wave, dl=literal_dl)
     assert np.abs(Ex - other[0]).max() > 0
+
+
+def test_three_level_kat_and_repaired_form(oracle_mod):
+    """The three-level KAT (the reference's ThreeLevel class as written) is
+    finite and moved by the gain sites; the repaired oscillators stay bounded
+    over 20 times as many steps, where the literal ones diverge."""
+    p, media, ids, wave, kw = gc.CASES_2D["three_literal"]()
+    lit = oracle_mod.run_orc2d(p, media, ids, wave, **kw)
+    assert all(np.isfinite(a).all() for a in lit)
+    plain = oracle_mod.run_orc2d(p, media, ids, wave)
+    assert np.abs(lit[0] - plain[0]).max() > 0
+    long_p = dict(p, nsteps=1200)
+    long_wave = np.concatenate([wave, np.zeros(1140)])
+    rep = dict(kw["three"], literal=0)
+    fixed = oracle_mod.run_orc2d(long_p, media, ids, long_wave, three=rep)
+    free = oracle_mod.run_orc2d(long_p, media, ids, long_wave)
+    assert all(np.isfinite(a).all() for a in fixed)
+    assert np.abs(fixed[0]).max() < 10 * np.abs(free[0]).max() + 1e-30
+    with np.errstate(all="ignore"):
+        wild = oracle_mod.run_orc2d(long_p, media, ids, long_wave, **kw)
+    assert not np.isfinite(wild[0]).all() or np.abs(wild[0]).max() > 1e6 * np.abs(free[0]).max()
