@@ -111,6 +111,7 @@ def lib():
             "cps_pml_init": ([P, C.POINTER(PmlParams)], I32),
             "cps_dl_init": ([P, C.POINTER(DlParams)], I32),
             "cps_drude_init": ([P, C.POINTER(DrudeParams)], I32),
+            "cps_grid_rasterize": ([P, I32, C.POINTER(Shape), I32], I32),
             "cps_three_init": ([P, C.POINTER(ThreeParams)], I32),
             "cps_three_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_op_three_polarization": ([P], I32), "cps_op_three_efield": ([P], I32),
@@ -175,11 +176,16 @@ def _dp(a):
     return a, a.ctypes.data_as(C.POINTER(C.c_double))
 
 
-def rasterize(nx, ny, nz, dx, dy, dz, shapes) -> np.ndarray:
-    """ID grid [i][j][k] of structure.txt shapes, as Structure::generate_mesh."""
+def _shape_array(shapes):
     arr = (Shape * max(1, len(shapes)))()
     for n, s in enumerate(shapes):
         arr[n] = Shape(SHAPE_TYPES[s.type], s.mat, s.theta, s.phi, s.psi, s.x0, s.y0, s.z0, s.a, s.b, s.c)
+    return arr
+
+
+def rasterize(nx, ny, nz, dx, dy, dz, shapes) -> np.ndarray:
+    """ID grid [i][j][k] of structure.txt shapes, as Structure::generate_mesh."""
+    arr = _shape_array(shapes)
     ids = np.zeros((nx + 1, ny + 1, nz + 1), dtype=np.uint8)
     _check(lib().cps_mesh_rasterize(nx, ny, nz, dx, dy, dz, len(shapes), arr, ids.ctypes.data, 0))
     return ids
@@ -233,12 +239,18 @@ class Grid:
 
     # --------------------------------------------------------- setup
     @classmethod
-    def from_deck(cls, dk, precision=FP32, ids: Optional[np.ndarray] = None, device=0, port_points_list=None):
+    def from_deck(cls, dk, precision=FP32, ids: Optional[np.ndarray] = None, device=0, port_points_list=None,
+                  device_raster=True):
+        """A grid set up from a deck; the shapes of a deck without an ID array are
+        rasterised on the device (device_raster=False: on the host, then uploaded)."""
         g = cls(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.dt, precision, device)
         g.set_media(dk.media)
-        if ids is None:
-            ids = dk.ids if dk.ids is not None else rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
-        g.upload_ids(ids)
+        if ids is None and dk.ids is None and device_raster:
+            g.rasterize(dk.shapes)
+        else:
+            if ids is None:
+                ids = dk.ids if dk.ids is not None else rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+            g.upload_ids(ids)
         if dk.pml:
             g.pml_init(dk.pml)
         if dk.dl:
@@ -263,6 +275,10 @@ class Grid:
         m = np.array(media, dtype=np.float64).reshape(-1, 4)
         cols = [_dp(m[:, c]) for c in range(4)]
         _check(self.L.cps_grid_set_media(self.h, len(m), *[c[1] for c in cols]))
+
+    def rasterize(self, shapes, keep=False):
+        """Rasterise structure.txt shapes into the grid's IDs on the device."""
+        _check(self.L.cps_grid_rasterize(self.h, len(shapes), _shape_array(shapes), 1 if keep else 0))
 
     def upload_ids(self, ids):
         ids = np.ascontiguousarray(ids, dtype=np.uint8)

@@ -35,6 +35,7 @@ SOURCES = {
     "kernels_batch.cu": [],
     "kernels_step.cu": [],
     "kernels_three.cu": ["--fmad=false"],
+    "raster.cu": ["--fmad=false"],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
     "noalloc.cu": [],

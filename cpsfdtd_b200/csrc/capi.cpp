@@ -878,6 +878,7 @@ extern "C" cps_status cps_grid_upload_ids(cps_grid *g, const uint8_t *ids)
     });
     REQUIRE(g->nmedia == 0 || maxid < g->nmedia, CPS_E_INVALID,
             "cps_grid_upload_ids: an ID has no medium (set the media first or extend them)");
+    g->ids_max = maxid;
     cps_status s = upload_raw(g, g->d_id, g->ids_dev.data(), g->ids_dev.size());
     if (s) return s;
     g->ids_set = true;

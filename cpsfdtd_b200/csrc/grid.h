@@ -116,6 +116,7 @@ struct cps_grid {
     uint2 *d_g_segm = nullptr;
     void *d_g_state = nullptr;
     // three-level gain (FP64 state on both precisions)
+    int ids_max = 0;              // largest material ID set
     bool three_on = false;
     cps::ThreeCoef tc{};
     int three_id = 5;

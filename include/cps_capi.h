@@ -215,6 +215,11 @@ CPS_API cps_status cps_grid_download_ids(const cps_grid *g, uint8_t *ids);
  * first unless keep != 0). */
 CPS_API cps_status cps_mesh_rasterize(int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
                                       int32_t nshapes, const cps_shape *shapes, uint8_t *ids, int32_t keep);
+/* The same rasterisation on the device, straight into the grid's IDs (the
+ * grid's cell sizes; the IDs are zeroed first unless keep != 0); the same
+ * cells get the same IDs as cps_mesh_rasterize + cps_grid_upload_ids.  Call it
+ * where cps_grid_upload_ids would be called. */
+CPS_API cps_status cps_grid_rasterize(cps_grid *g, int32_t nshapes, const cps_shape *shapes, int32_t keep);
 
 /* ---- physics modules (call after media and IDs are set) ---- */
 CPS_API cps_status cps_pml_init(cps_grid *g, const cps_pml_params *p);

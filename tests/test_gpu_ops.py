@@ -104,3 +104,24 @@ def test_errors_are_reported():
         g.pml_init(dict(npml=[4, 5, 4, 4, 4, 4], m=3, malp=1, kapmax=5, sig_ratio=1, alpmax=0.05))
     with pytest.raises(cps.CpsError):
         g.port_add(np.array([[0, 0, 17]]))
+
+
+@pytest.mark.parametrize("name", ["shapes_pec", "c2", "c1"])
+def test_device_rasterisation_equals_host(name):
+    """cps_grid_rasterize gives every cell the ID cps_mesh_rasterize gives it:
+    axis-aligned and rotated cuboids, cylinders, ellipsoids, multi shapes."""
+    import cpsfdtd_b200 as cps
+    import golden.golden_cases as gc
+    dk = {"shapes_pec": gc.shapes_pec, "c2": lambda: decks.config2(n=96, steps=1, nfreq=1),
+          "c1": lambda: decks.config1(n=64, steps=1)}[name]()
+    host = cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    g = cps.Grid(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.dt, cps.FP32)
+    g.set_media(dk.media)
+    g.rasterize(dk.shapes)
+    assert np.array_equal(g.download_ids(), host)
+    g.rasterize(dk.shapes[:1], keep=True)  # keep: the first shape painted again on top
+    again = cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, list(dk.shapes) + list(dk.shapes[:1]))
+    assert np.array_equal(g.download_ids(), again)
+    bad = decks.Shape(len(dk.media), "cuboid", 0, 0, 0, dk.dx, dk.dx, dk.dx)
+    with pytest.raises(cps.CpsError):
+        g.rasterize([bad])
