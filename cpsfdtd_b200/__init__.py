@@ -112,6 +112,7 @@ def lib():
             "cps_dl_init": ([P, C.POINTER(DlParams)], I32),
             "cps_drude_init": ([P, C.POINTER(DrudeParams)], I32),
             "cps_grid_rasterize": ([P, I32, C.POINTER(Shape), I32], I32),
+            "cps_deck_load": ([C.c_char_p, I32, C.POINTER(P)], I32),
             "cps_three_init": ([P, C.POINTER(ThreeParams)], I32),
             "cps_three_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_op_three_polarization": ([P], I32), "cps_op_three_efield": ([P], I32),
@@ -225,6 +226,23 @@ class Grid:
         self.shape3 = (nx + 1, ny + 1, nz + 1)
         self.precision = precision
         self.ports = []  # (npts, ncomp, nfreq)
+
+    @classmethod
+    def from_deck_dir(cls, path, precision=FP32):
+        """A grid from a directory of the reference's deck files (cps_deck_load);
+        its ports carry no DFT and it has no sources until they are added."""
+        g = cls.__new__(cls)
+        g.L = lib()
+        g.h = C.c_void_p()
+        _check(g.L.cps_deck_load(os.fsencode(path), precision, C.byref(g.h)))
+        info = GridDesc()
+        _check(g.L.cps_grid_info(g.h, C.byref(info)))
+        g.desc = info
+        g.dt = info.dt
+        g.shape3 = (info.nx + 1, info.ny + 1, info.nz + 1)
+        g.precision = precision
+        g.ports = []
+        return g
 
     def close(self):
         if getattr(self, "h", None) and self.h.value:

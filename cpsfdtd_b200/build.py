@@ -36,6 +36,7 @@ SOURCES = {
     "kernels_step.cu": [],
     "kernels_three.cu": ["--fmad=false"],
     "raster.cu": ["--fmad=false"],
+    "deck_load.cpp": [],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
     "noalloc.cu": [],

@@ -42,6 +42,7 @@
  *   cps_op_tfsf_h / tfsf_e .... TF_SF::UpdateHField / UpdateEField and the face variants
  *                               (TF_SF.cpp:1201-1410, 988-1199)
  *   cps_op_port_sample ........ SphericalPort/PlainPort::Update_Fields_on_Port (Ports.cpp:88-99, 342-353)
+ *   cps_deck_load ............. main.cpp:110-262's object construction from the resourses/ decks
  *   cps_step .................. one pass of the loop body of main.cpp:267-344
  *   cps_grid_set_record ....... (no counterpart) runs a step's cps_op_* calls, made in
  *                               main.cpp's order, as one fused step
@@ -220,6 +221,15 @@ CPS_API cps_status cps_mesh_rasterize(int32_t nx, int32_t ny, int32_t nz, double
  * cells get the same IDs as cps_mesh_rasterize + cps_grid_upload_ids.  Call it
  * where cps_grid_upload_ids would be called. */
 CPS_API cps_status cps_grid_rasterize(cps_grid *g, int32_t nshapes, const cps_shape *shapes, int32_t keep);
+
+/* A grid from a directory of the reference's deck files (material.txt,
+ * structure.txt; CFS_PML.txt, DrudeLorentz.txt or Drude.txt, FourLevelLaser.txt
+ * or ThreeLevel.txt, TF_SF.txt, port0.txt, port1.txt, ... when present), set up
+ * through the drop-in classes' parsing (cpsfdtd_classes.hpp).  A malformed or
+ * missing required deck gives CPS_E_INVALID with the file named; a failing
+ * set-up call gives that call's status.  Port DFTs and sources (main.cpp code
+ * in the reference) are added by the caller.  The caller destroys *out. */
+CPS_API cps_status cps_deck_load(const char *dir, int32_t precision, cps_grid **out);
 
 /* ---- physics modules (call after media and IDs are set) ---- */
 CPS_API cps_status cps_pml_init(cps_grid *g, const cps_pml_params *p);

@@ -36,9 +36,15 @@
 
 namespace cpsfdtd_detail {
 
+// a failed C-ABI call: the message and the call's status
+struct call_error : std::runtime_error {
+    cps_status code;
+    call_error(const std::string &m, cps_status c) : std::runtime_error(m), code(c) {}
+};
+
 inline void check(cps_status s, const char *what)
 {
-    if (s != CPS_OK) throw std::runtime_error(std::string(what) + ": " + cps_last_error());
+    if (s != CPS_OK) throw call_error(std::string(what) + ": " + cps_last_error(), s);
 }
 
 // the lines of a deck; a missing file is an error (the reference reads zeros)
@@ -219,6 +225,14 @@ public:
     {
         if (!grid_) throw std::runtime_error("the grid exists after InitializeBasicFDTDCoefficients");
         return grid_;
+    }
+
+    // hand the device grid to the caller, who destroys it (cps_grid_destroy)
+    cps_grid *release_grid()
+    {
+        cps_grid *g = grid();
+        grid_ = nullptr;
+        return g;
     }
 
     double Lx = 0, Ly = 0, Lz = 0;

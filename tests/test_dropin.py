@@ -95,3 +95,43 @@ def test_dropin_matches_oracle(tmp_path, oracle_mod, case, record):
         assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max() + 1e-300
         ijk = np.loadtxt(str(out / f"portP{q}.txt"), dtype=np.int64).reshape(-1, 3)
         assert np.array_equal(ijk, p)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["dispersive", "drude", "laser", "three"])
+def test_deck_load_equals_grid_from_deck(tmp_path, case):
+    """cps_deck_load (the drop-in classes' parsing, as one C call) builds the grid
+    Grid.from_deck builds from the same deck: equal fields after 30 steps."""
+    import cpsfdtd_b200 as cps
+    if case in ("dispersive", "drude"):
+        dk = decks.config2(n=36, steps=30, nfreq=0)
+        if case == "drude":
+            dk.dl = decks.drude_as_dl(decks.drude_params_metal())
+    else:
+        dk = decks.config3(n=36, steps=30, nfreq=0, port=False)
+        if case == "three":
+            dk.gain = None
+            dk.three = decks.three_params_laser()
+    dk.sources = []  # main.cpp code in the reference, not a deck
+    for p in dk.ports:
+        p.dft_freqs = None
+    deck = tmp_path / "deck"
+    dk.write(str(deck))
+    a = cps.Grid.from_deck_dir(str(deck), cps.FP64)
+    b = cps.Grid.from_deck(dk, cps.FP64)
+    assert a.shape3 == b.shape3 and a.dt == b.dt
+    a.set_step(1)
+    b.set_step(1)
+    a.step(30, cps.FUSED)
+    b.step(30, cps.FUSED)
+    for c in range(6):
+        assert np.array_equal(a.field(c), b.field(c)), c
+    a.close()
+    b.close()
+
+
+def test_deck_load_reports_bad_decks(tmp_path):
+    import cpsfdtd_b200 as cps
+    with pytest.raises(cps.CpsError) as e:
+        cps.Grid.from_deck_dir(str(tmp_path / "nothing"), cps.FP32)
+    assert "material.txt" in str(e.value)
