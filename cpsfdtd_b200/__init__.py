@@ -113,6 +113,9 @@ def lib():
             "cps_drude_init": ([P, C.POINTER(DrudeParams)], I32),
             "cps_grid_rasterize": ([P, I32, C.POINTER(Shape), I32], I32),
             "cps_deck_load": ([C.c_char_p, I32, C.POINTER(P)], I32),
+            "cps_field_slice": ([P, I32, I32, I32, dp], I32),
+            "cps_image_png": ([C.c_char_p, I32, I32, dp, D, D], I32),
+            "cps_png_rgb": ([C.c_char_p, I32, I32, C.c_void_p], I32),
             "cps_three_init": ([P, C.POINTER(ThreeParams)], I32),
             "cps_three_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_op_three_polarization": ([P], I32), "cps_op_three_efield": ([P], I32),
@@ -190,6 +193,13 @@ def rasterize(nx, ny, nz, dx, dy, dz, shapes) -> np.ndarray:
     ids = np.zeros((nx + 1, ny + 1, nz + 1), dtype=np.uint8)
     _check(lib().cps_mesh_rasterize(nx, ny, nz, dx, dy, dz, len(shapes), arr, ids.ctypes.data, 0))
     return ids
+
+
+def image_png(path, values, cmin, cmax):
+    """PNG of a 2-D array values[x][y] through the reference OutImage's colour map."""
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    _check(lib().cps_image_png(os.fsencode(path), v.shape[0], v.shape[1], v.ctypes.data_as(C.POINTER(C.c_double)),
+                               float(cmin), float(cmax)))
 
 
 def port_points(deck, port) -> np.ndarray:
@@ -410,6 +420,15 @@ class Grid:
     def field(self, comp):
         out = np.empty(self.shape3, dtype=np.float64)
         _check(self.L.cps_field_download(self.h, comp, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def slice(self, what, axis, index):
+        """One plane of component `what` (0..5) or of |E|^2 (6), cut on the device:
+        [u][v] with (u, v) = (j, k), (i, k) or (i, j) for axis 0, 1, 2."""
+        nu = (self.shape3[1] if axis == 0 else self.shape3[0])
+        nv = (self.shape3[1] if axis == 2 else self.shape3[2])
+        out = np.empty((nu, nv))
+        _check(self.L.cps_field_slice(self.h, what, axis, index, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
     def fields(self):

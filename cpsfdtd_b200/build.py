@@ -37,6 +37,7 @@ SOURCES = {
     "kernels_three.cu": ["--fmad=false"],
     "raster.cu": ["--fmad=false"],
     "deck_load.cpp": [],
+    "image.cu": [],
     "batch.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
     "noalloc.cu": [],

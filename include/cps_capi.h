@@ -47,6 +47,7 @@
  *   cps_grid_set_record ....... (no counterpart) runs a step's cps_op_* calls, made in
  *                               main.cpp's order, as one fused step
  *   cps_field_download/upload . direct access to Field::Ex..Hz (Fields.h:28-33)
+ *   cps_field_slice, cps_image_png  OutImage (OutImage.h:22-45) without a display
  *   cps_port_read ............. Port_Points::Ex..Hz after Update_Fields_on_Port
  *   cps_port_dft_read / flux .. (no reference counterpart: running FP64 DFT of the port samples)
  */
@@ -318,6 +319,17 @@ CPS_API cps_status cps_grid_record_stats(const cps_grid *g, int64_t *fused_steps
 CPS_API cps_status cps_field_download(cps_grid *g, int32_t comp, double *out);
 CPS_API cps_status cps_field_upload(cps_grid *g, int32_t comp, const double *in);
 CPS_API cps_status cps_field_download_f32(cps_grid *g, int32_t comp, float *out);
+/* one plane of a field component (what 0..5) or of |E|^2 (what 6), cut on the
+ * device: out[u][v] FP64 with (u, v) = (j, k) for a plane of constant x (axis
+ * 0), (i, k) for y (axis 1), (i, j) for z (axis 2) */
+CPS_API cps_status cps_field_slice(cps_grid *g, int32_t what, int32_t axis, int32_t index, double *out);
+/* Headless stand-in for OutImage::plot_save (OutImage.cpp:140-200): an RGB
+ * PNG of values[x][y] (nx x ny) through OutImage's colour map between cmin and
+ * cmax (no display, no image library) */
+CPS_API cps_status cps_image_png(const char *path, int32_t nx, int32_t ny, const double *values, double cmin,
+                                 double cmax);
+/* an 8-bit RGB PNG of rgb[y][x][3] */
+CPS_API cps_status cps_png_rgb(const char *path, int32_t nx, int32_t ny, const uint8_t *rgb);
 /* reset fields, auxiliary state, port samples and DFT accumulators to zero
  * (initial populations for gain) and the step index to n0 */
 CPS_API cps_status cps_grid_reset(cps_grid *g, int64_t n0);

@@ -23,6 +23,7 @@
 #pragma once
 
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -623,6 +624,54 @@ private:
     }
     cps_grid *g_ = nullptr;
     std::vector<double> tab_;
+};
+
+// OutImage.h:22-45 without a display: the reference draws through CImg and
+// an X11 window; here plot_save and structure_plot_save write the same PNG
+// files (OutImage.cpp:140-216) and plot() has nothing to show.
+class OutImage {
+public:
+    OutImage(int N_x, int N_y, int save_modulus, double cmap_min, double cmap_max, const char *file_name_base)
+        : savemodulus(save_modulus > 0 ? save_modulus : 1), Nx(N_x), Ny(N_y), cmapmin(cmap_min), cmapmax(cmap_max),
+          filenamebase(file_name_base ? file_name_base : "")
+    {
+        cmapmid = (cmapmax + cmapmin) / 2.0;
+        cmapthird = (cmapmax + cmapmin) / 3.0;
+        cmap2third = (cmapmax + cmapthird) / 2.0;
+        static const short table[10][3] = {{254, 254, 254}, {254, 0, 0},   {0, 0, 254},   {0, 254, 0},   {0, 0, 0},
+                                           {254, 254, 0},   {0, 254, 254}, {254, 0, 254}, {127, 0, 254}, {0, 127, 254}};
+        for (int q = 0; q < color_table_length; ++q)
+            for (int c = 0; c < 3; ++c) color_table[q][c] = table[q][c];
+    }
+    void plot_save(double **dD, int time_step)
+    {
+        if (time_step % savemodulus != 0) return;
+        std::vector<double> v((size_t)Nx * Ny);
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < Ny; ++j) v[(size_t)i * Ny + j] = dD[i][j];
+        char name[512];
+        snprintf(name, sizeof(name), "%s%06d.png", filenamebase.c_str(), time_step / savemodulus);
+        cpsfdtd_detail::check(cps_image_png(name, Nx, Ny, v.data(), cmapmin, cmapmax), "plot_save");
+    }
+    void structure_plot_save(short **dD)
+    {
+        std::vector<uint8_t> rgb((size_t)Nx * Ny * 3);
+        for (int i = 0; i < Nx; ++i)
+            for (int j = 0; j < Ny; ++j) {
+                const int id = dD[i][j];
+                if (id < 0 || id >= color_table_length) throw std::runtime_error("structure_plot_save: ID without a colour");
+                for (int c = 0; c < 3; ++c) rgb[((size_t)j * Nx + i) * 3 + c] = (uint8_t)color_table[id][c];
+            }
+        const std::string name = filenamebase + "_structure.png";
+        cpsfdtd_detail::check(cps_png_rgb(name.c_str(), Nx, Ny, rgb.data()), "structure_plot_save");
+    }
+    void plot() {}
+    void plot(double **, int) {}
+
+    int savemodulus, Nx, Ny, color_table_length = 10;
+    double cmapmin, cmapmax, cmapmid, cmapthird, cmap2third;
+    short color_table[10][3];
+    std::string filenamebase;
 };
 
 // Ports.h:20-27
