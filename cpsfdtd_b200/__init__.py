@@ -116,6 +116,7 @@ def lib():
             "cps_field_slice": ([P, I32, I32, I32, dp], I32),
             "cps_image_png": ([C.c_char_p, I32, I32, dp, D, D], I32),
             "cps_png_rgb": ([C.c_char_p, I32, I32, C.c_void_p], I32),
+            "cps_grid_energy": ([P, C.POINTER(D), C.POINTER(D)], I32),
             "cps_three_init": ([P, C.POINTER(ThreeParams)], I32),
             "cps_three_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_op_three_polarization": ([P], I32), "cps_op_three_efield": ([P], I32),
@@ -430,6 +431,12 @@ class Grid:
         out = np.empty((nu, nv))
         _check(self.L.cps_field_slice(self.h, what, axis, index, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
+
+    def energy(self):
+        """(electric, magnetic) energy in joules, summed on the device"""
+        e, h = C.c_double(), C.c_double()
+        _check(self.L.cps_grid_energy(self.h, C.byref(e), C.byref(h)))
+        return e.value, h.value
 
     def fields(self):
         return [self.field(c) for c in range(6)]

@@ -839,6 +839,8 @@ extern "C" cps_status cps_grid_set_media(cps_grid *g, int32_t n, const double *e
         g->bE[i] = (2.0 * dt) / (2.0 * kEps0 * epsR[i] + sig[i] * dt);
         g->aH[i] = (2.0 * kMu0 * muR[i] - sigM[i] * dt) / (2.0 * kMu0 * muR[i] + sigM[i] * dt);
         g->bH[i] = (2.0 * dt) / (2.0 * kMu0 * muR[i] + sigM[i] * dt);
+        g->eps_r[i] = epsR[i];
+        g->mu_r[i] = muR[i];
     }
     g->nmedia = n;
     std::vector<double> t(1024, 0.0);

@@ -88,6 +88,7 @@ struct cps_grid {
     std::vector<uint8_t> ids_dev;  // host copy in device order
     bool ids_set = false;
     int nmedia = 0;
+    double eps_r[256] = {}, mu_r[256] = {};  // relative permittivity and permeability per medium
     double aE[256] = {}, bE[256] = {}, aH[256] = {}, bH[256] = {};
     void *d_media = nullptr;  // aE bE aH bH, 256 each, of T
     std::vector<double> st[12];

@@ -39,6 +39,43 @@ __global__ void k_slice(FieldView<T> f, int what, int axis, int index, int nu, i
     out[q] = r;
 }
 
+struct MediaTable {
+    double eps[256], mu[256];  // eps0 epsR and mu0 muR per medium
+};
+
+// electric and magnetic energy sums, FP64, one atomic pair per block
+template <typename T>
+__global__ void __launch_bounds__(256) k_energy(FieldView<T> f, MediaTable m, double *out)
+{
+    const Dims &d = f.d;
+    const int64_t n = (int64_t)(d.nx + 1) * (d.ny + 1) * (d.nz + 1);
+    double we = 0.0, wh = 0.0;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % (d.nx + 1)), j = (int)((q / (d.nx + 1)) % (d.ny + 1)),
+                  k = (int)(q / ((int64_t)(d.nx + 1) * (d.ny + 1)));
+        const int64_t g = d.idx(i, j, k);
+        const int id = f.id[g];
+        const double ex = (double)f.Ex[g], ey = (double)f.Ey[g], ez = (double)f.Ez[g];
+        const double hx = (double)f.Hx[g], hy = (double)f.Hy[g], hz = (double)f.Hz[g];
+        we += m.eps[id] * (ex * ex + ey * ey + ez * ez);
+        wh += m.mu[id] * (hx * hx + hy * hy + hz * hz);
+    }
+    __shared__ double se[8], sh[8];
+    for (int o = 16; o > 0; o >>= 1) {
+        we += __shfl_down_sync(0xffffffffu, we, o);
+        wh += __shfl_down_sync(0xffffffffu, wh, o);
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) { se[w] = we; sh[w] = wh; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) { a += se[q]; b += sh[q]; }
+        atomicAdd(&out[0], a);
+        atomicAdd(&out[1], b);
+    }
+}
+
 struct CrcTable {
     uint32_t t[256];
     CrcTable()
@@ -175,4 +212,35 @@ extern "C" cps_status cps_image_png(const char *path, int32_t nx, int32_t ny, co
             else { px[0] = 254; px[1] = 254; px[2] = (uint8_t)temp; }
         }
     return cps_png_rgb(path, nx, ny, rgb.data());
+}
+
+extern "C" cps_status cps_grid_energy(cps_grid *g, double *electric, double *magnetic)
+{
+    REQUIRE(g && electric && magnetic, CPS_E_INVALID, "cps_grid_energy: NULL argument");
+    REQUIRE(g->nmedia > 0 && g->ids_set, CPS_E_STATE, "cps_grid_energy: media and IDs are not set");
+    cps_status s = flush_recorded(g);
+    if (s) return s;
+    MediaTable m;
+    for (int q = 0; q < 256; ++q) {
+        m.eps[q] = kEps0 * (q < g->nmedia ? g->eps_r[q] : 1.0);
+        m.mu[q] = kMu0 * (q < g->nmedia ? g->mu_r[q] : 1.0);
+    }
+    double *d_out = nullptr;
+    if ((s = dalloc(g, (void **)&d_out, 2 * sizeof(double)))) return s;
+    double h[2] = {0.0, 0.0};
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 2 * sizeof(double), g->stream);
+    if (e == cudaSuccess) {
+        if (g->fp32) k_energy<float><<<148 * 8, 256, 0, g->stream>>>(field_view<float>(g), m, d_out);
+        else k_energy<double><<<148 * 8, 256, 0, g->stream>>>(field_view<double>(g), m, d_out);
+        g->launches++;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d_out, sizeof(h), cudaMemcpyDeviceToHost, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    dfree(g, d_out);
+    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("cps_grid_energy: ") + cudaGetErrorString(e));
+    const double dV = g->desc.dx * g->desc.dy * g->desc.dz;
+    *electric = 0.5 * h[0] * dV;
+    *magnetic = 0.5 * h[1] * dV;
+    return CPS_OK;
 }

@@ -328,6 +328,11 @@ CPS_API cps_status cps_field_slice(cps_grid *g, int32_t what, int32_t axis, int3
  * cmax (no display, no image library) */
 CPS_API cps_status cps_image_png(const char *path, int32_t nx, int32_t ny, const double *values, double cmin,
                                  double cmax);
+/* electromagnetic energy in the grid (no reference counterpart): electric
+ * 0.5 sum eps0 epsR |E|^2 dV and magnetic 0.5 sum mu0 muR |H|^2 dV over all
+ * cells, each cell's medium for both (dispersive and gain polarisation energy
+ * not included), summed in FP64 on the device */
+CPS_API cps_status cps_grid_energy(cps_grid *g, double *electric, double *magnetic);
 /* an 8-bit RGB PNG of rgb[y][x][3] */
 CPS_API cps_status cps_png_rgb(const char *path, int32_t nx, int32_t ny, const uint8_t *rgb);
 /* reset fields, auxiliary state, port samples and DFT accumulators to zero

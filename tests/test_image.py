@@ -123,3 +123,25 @@ def test_field_slice_equals_download():
                 got = g.slice(what, axis, index)
                 assert np.allclose(got, want, rtol=1e-12, atol=0) if what == 6 else np.array_equal(got, want)
         g.close()
+
+
+@pytest.mark.gpu
+def test_grid_energy_equals_host_sum():
+    import cpsfdtd_b200 as cps
+    from cpsfdtd_b200 import decks
+    dk = decks.config1(n=40, steps=1)
+    eps0, mu0 = 8.8541878176e-12, 1.2566370614e-6
+    for prec in (cps.FP32, cps.FP64):
+        g = cps.Grid.from_deck(dk, prec)
+        g.step(30, cps.FUSED)
+        ids = g.download_ids()
+        epsr = np.array([m[0] for m in dk.media])[ids]
+        mur = np.array([m[1] for m in dk.media])[ids]
+        f = [g.field(c) for c in range(6)]
+        dv = dk.dx * dk.dy * dk.dz
+        want_e = 0.5 * dv * eps0 * np.sum(epsr * (f[0] ** 2 + f[1] ** 2 + f[2] ** 2))
+        want_h = 0.5 * dv * mu0 * np.sum(mur * (f[3] ** 2 + f[4] ** 2 + f[5] ** 2))
+        got_e, got_h = g.energy()
+        assert want_e > 0 and want_h > 0
+        assert abs(got_e - want_e) <= 1e-12 * want_e and abs(got_h - want_h) <= 1e-12 * want_h
+        g.close()
