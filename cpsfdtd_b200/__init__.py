@@ -132,7 +132,7 @@ def lib():
             "cps_port_read": ([P, I32, dp], I32), "cps_port_dft_read": ([P, I32, dp], I32),
             "cps_port_flux": ([P, I32, C.c_char, dp], I32),
             "cps_grid_set_step": ([P, I64], I32), "cps_grid_get_step": ([P, C.POINTER(I64)], I32),
-            "cps_step": ([P, I32, I32], I32),
+            "cps_step": ([P, I32, I32], I32), "cps_grid_set_chunked": ([P, I32], I32),
             "cps_op_h_bulk": ([P], I32), "cps_op_e_bulk": ([P], I32), "cps_op_h_pml": ([P], I32),
             "cps_op_e_pml": ([P], I32), "cps_op_dl": ([P], I32), "cps_op_gain_polarization": ([P], I32),
             "cps_op_gain_efield": ([P], I32), "cps_op_gain_populations": ([P], I32),
@@ -400,6 +400,10 @@ class Grid:
 
     def sync(self):
         _check(self.L.cps_synchronize(self.h))
+
+    def set_chunked(self, on):
+        """fused steps of large grids as graph-replayed one-grid batch chunks (default on)"""
+        _check(self.L.cps_grid_set_chunked(self.h, 1 if on else 0))
 
     def reset(self, n0=1):
         _check(self.L.cps_grid_reset(self.h, n0))

@@ -749,6 +749,7 @@ extern "C" cps_status cps_grid_destroy(cps_grid *g)
 {
     if (!g) return CPS_OK;
     cudaSetDevice(g->desc.device);
+    if (g->solo) cps_batch_destroy(g->solo);
     for (auto &a : g->owned) cudaFreeAsync(a.first, g->stream);
     g->owned.clear();
     if (g->stream) cudaStreamSynchronize(g->stream);
@@ -819,6 +820,10 @@ extern "C" cps_status cps_synchronize(cps_grid *g)
 {
     REQUIRE(g, CPS_E_INVALID, "NULL grid");
     FLUSH_RECORDED(g);
+    if (g->solo) {
+        cps_status s = cps_batch_synchronize(g->solo);
+        if (s) return s;
+    }
     CK(cudaStreamSynchronize(g->stream));
     return check_device_error(g);
 }
@@ -1529,6 +1534,52 @@ extern "C" cps_status cps_grid_get_step(const cps_grid *g, int64_t *n)
     return CPS_OK;
 }
 
+namespace {
+// grids at or above this size step the fused path as chunks of a one-grid
+// batch: the batch launches their sweeps per grid inside CUDA-graph-replayed
+// chunks and the rest of the step in batched launches, with results equal to
+// the direct launches
+constexpr int64_t kSoloMinCells = 4 << 20;
+
+bool solo_eligible(const cps_grid *g)
+{
+    return g->chunked && g->timing_stride == 0 && g->sweep_mode == 0 && !g->three_on &&
+           (g->shape.by == 4 || g->shape.by == 8) && g->d.px >= 64 && g->d.ny >= 8 && g->d.nz >= 2 &&
+           (int64_t)g->d.nx * g->d.ny * g->d.nz >= kSoloMinCells;
+}
+
+cps_status solo_step(cps_grid *g, int32_t nsteps)
+{
+    cps_status s;
+    if (!g->solo) {
+        if ((s = cps_batch_create(g->desc.precision, &g->solo))) return s;
+        if ((s = cps_batch_add(g->solo, g))) {
+            cps_batch_destroy(g->solo);
+            g->solo = nullptr;
+            return s;
+        }
+    }
+    int32_t rows = 0, planes = 0, pers = 0;
+    if ((s = cps_batch_get_tile(g->solo, &rows, &planes, &pers))) return s;
+    if ((rows != g->shape.by || planes != g->shape.kc || pers != 0) &&
+        (s = cps_batch_set_tile(g->solo, g->shape.by, g->shape.kc, 0)))
+        return s;
+    int64_t l0 = 0, l1 = 0;
+    cps_batch_launch_count(g->solo, &l0);
+    s = cps_batch_step(g->solo, nsteps);
+    cps_batch_launch_count(g->solo, &l1);
+    g->launches += l1 - l0;
+    return s;
+}
+}  // namespace
+
+extern "C" cps_status cps_grid_set_chunked(cps_grid *g, int32_t on)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    g->chunked = on != 0;
+    return CPS_OK;
+}
+
 extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
 {
     cps_status s = need_setup(g);
@@ -1538,6 +1589,7 @@ extern "C" cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path)
     REQUIRE(path == CPS_PATH_PLAIN || path == CPS_PATH_FUSED || path == CPS_PATH_ONEPASS, CPS_E_INVALID,
             "cps_step: unknown path");
     CK(cudaSetDevice(g->desc.device));
+    if (path == CPS_PATH_FUSED && nsteps > 0 && solo_eligible(g)) return solo_step(g, nsteps);
     return g->fp32 ? step_T<float>(g, nsteps, path) : step_T<double>(g, nsteps, path);
 }
 

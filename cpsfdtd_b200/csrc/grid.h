@@ -174,6 +174,9 @@ struct cps_grid {
     std::vector<cudaEvent_t> ev;
     int ev_used = 0;
     std::vector<std::pair<void *, size_t>> owned;  // every device allocation and its size
+    // cps_step on the fused path as graph-replayed chunks of a one-grid batch
+    bool chunked = true;
+    cps_batch *solo = nullptr;
     // op recorder (cps_grid_set_record)
     bool record = false;
     std::vector<cps::RecOp> pending;

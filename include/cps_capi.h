@@ -278,6 +278,11 @@ CPS_API cps_status cps_grid_get_step(const cps_grid *g, int64_t *n);
  * CPML H, E bulk, Drude-Lorentz, gain (P, E, N), TF/SF E, sources, CPML E,
  * port sampling.  Asynchronous on the grid's stream. */
 CPS_API cps_status cps_step(cps_grid *g, int32_t nsteps, int32_t path);
+/* On (default): cps_step on the fused path runs grids of 4 Mi cells or more
+ * as chunks of a one-grid batch (the batch's CUDA-graph-replayed chunks; the
+ * results are the direct launches' bit for bit), except while per-step timing
+ * (cps_grid_set_timing) is on; off: one launch sequence per step. */
+CPS_API cps_status cps_grid_set_chunked(cps_grid *g, int32_t on);
 
 /* ---- single reference routines (one launch each, enqueued on the grid's stream) ---- */
 CPS_API cps_status cps_op_h_bulk(cps_grid *g);

@@ -183,3 +183,24 @@ def test_batch_with_a_large_member_equals_alone():
     b.sync()
     for n, g in enumerate(gs):
         _same(ref[n], _state(g), f"member {n}")
+
+
+def test_chunked_fused_steps_equal_direct_launches():
+    """A grid of 4 Mi cells or more steps the fused path as one-grid batch
+    chunks (graph replay); results equal the direct launches bit for bit,
+    across chunk boundaries, a reset and the port DFTs."""
+    import cpsfdtd_b200 as cps
+    dk = decks.config2(n=164, steps=1, nfreq=3)
+    a, b = _grid(dk, cps.FP32), _grid(dk, cps.FP32)
+    b.set_chunked(False)
+    for g in (a, b):
+        g.step(70, cps.FUSED)
+        g.step(64, cps.FUSED)
+        g.step(3, cps.FUSED)
+    ra, rb = _state(a), _state(b)
+    _same(rb, ra, "chunked")
+    for g in (a, b):
+        g.reset(1)
+        g.step(65, cps.FUSED)
+    _same(_state(b), _state(a), "after reset")
+    assert a.launches() > 0
