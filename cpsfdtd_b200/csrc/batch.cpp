@@ -104,6 +104,11 @@ struct cps_batch {
     int nports = 0;
     int64_t cells = 0;
     std::vector<int> big;  // members stepped with their own sweep launches
+    // side streams the per-member sweep launches fan out over (member q on
+    // side[q % side.size()]), so that several members' sweeps run at once
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_done;
+    cudaEvent_t fork = nullptr;
     // graphs per chunk length
     std::map<int, std::pair<cudaGraphExec_t, int64_t>> graphs;  // executable and its kernel count
     std::map<int, int> direct;  // chunk lengths launched directly since the last rebuild
@@ -180,6 +185,50 @@ cps_status sync_grid_streams_out(cps_batch *b)
     return CPS_OK;
 }
 
+// Side streams for the per-member sweep launches: up to kSideStreams, made
+// outside any capture when the tables are rebuilt.
+constexpr size_t kSideStreams = 8;
+
+cps_status ensure_side_streams(cps_batch *b)
+{
+    const size_t want = b->big.size() > 1 ? std::min(kSideStreams, b->big.size()) : 0;
+    if (want && !b->fork) CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    while (b->side.size() < want) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            cudaStreamDestroy(st);
+            CK(e);
+        }
+        b->side.push_back(st);
+        b->side_done.push_back(ev);
+    }
+    return CPS_OK;
+}
+
+// The per-member sweeps of one phase: on the batch stream one after another,
+// or fanned out over the side streams between an event fork and join (which a
+// capture records as graph edges).
+template <typename F>
+void per_member(cps_batch *b, F &&launch)
+{
+    if (b->big.empty()) return;
+    const size_t ns = b->big.size() > 1 ? std::min(b->side.size(), b->big.size()) : 0;
+    if (ns == 0) {
+        for (int gi : b->big) launch(gi, b->stream);
+        return;
+    }
+    cudaEventRecord(b->fork, b->stream);
+    for (size_t k = 0; k < ns; ++k) cudaStreamWaitEvent(b->side[k], b->fork, 0);
+    for (size_t q = 0; q < b->big.size(); ++q) launch(b->big[q], b->side[q % ns]);
+    for (size_t k = 0; k < ns; ++k) {
+        cudaEventRecord(b->side_done[k], b->side[k]);
+        cudaStreamWaitEvent(b->stream, b->side_done[k], 0);
+    }
+}
+
 template <typename T>
 cps_status rebuild_T(cps_batch *b)
 {
@@ -231,7 +280,7 @@ cps_status rebuild_T(cps_batch *b)
         const int nbx = cdiv_i(d.nx, 32), nby = cdiv_i(d.ny, by), nbz = cdiv_i(d.nz, kc);
         // a grid that fills the device alone gets its own sweep launches (tensor
         // maps as kernel parameters); the rest of its step stays batched
-        const bool is_big = (int64_t)d.nx * d.ny * d.nz >= kBigCells;
+        const bool is_big = b->persistent == 2 || (int64_t)d.nx * d.ny * d.nz >= kBigCells;
         if (is_big) b->big.push_back((int)gi);
         for (int bz = 0; bz < nbz && !is_big; ++bz)
             for (int yb = 0; yb < nby; ++yb)
@@ -307,13 +356,14 @@ cps_status rebuild_T(cps_batch *b)
         if ((s = upload_vec(b, &b->d_tiles[c], tiles[c]))) return s;
         b->ntiles[c] = (int)tiles[c].size();
         b->nblocks[c] = b->ntiles[c];
-        if (b->persistent && b->ntiles[c] > 0) {
+        if (b->persistent == 1 && b->ntiles[c] > 0) {
             const bool eside = c >= kE0;
             const int cls = eside ? c - kE0 : (c == kHPml ? 1 : 0);
             const int per_sm = batch_blocks_per_sm<T>(by, eside, cls);
             b->nblocks[c] = std::min(b->ntiles[c], per_sm * nsm);
         }
     }
+    if ((s = ensure_side_streams(b))) return s;
     if ((s = upload_vec(b, &b->d_dl, dl))) return s;
     b->ndl = (int)dl.size();
     for (int side = 0; side < 2; ++side) {
@@ -347,19 +397,19 @@ int64_t enqueue_chunk(cps_batch *b, int S)
     for (int s = 0; s < S; ++s) {
         launch_h_batch<T>(G, b->d_tiles[kHInt], b->ntiles[kHInt], b->nblocks[kHInt], b->by, false, b->d_err, st);
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
-        for (int gi : b->big) {
+        per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
-            launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, st);
-        }
+            launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, ms);
+        });
         launch_inject_batch<T>(G, b->d_inj[1], b->ninj[1], 1, s, st);
         for (int c = 0; c < 8; ++c)
             launch_e_batch<T>(G, b->d_tiles[kE0 + c], b->ntiles[kE0 + c], b->nblocks[kE0 + c], b->by, c, b->d_err, st);
         launch_dl_batch<T>(G, b->d_dl, b->ndl, st);
-        for (int gi : b->big) {
+        per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
             launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
-                            FusedShape{b->by, b->kc}, b->d_err, st);
-        }
+                            FusedShape{b->by, b->kc}, b->d_err, ms);
+        });
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);
         launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, st);
@@ -484,7 +534,7 @@ bool cache_lookup(const char *path, const std::string &key, int *by, int *kc, in
         std::string k;
         int a, c, p;
         double ms;
-        if (ss >> k >> a >> c >> p >> ms && k == key && (a == 4 || a == 8) && c >= 1 && (p == 0 || p == 1)) {
+        if (ss >> k >> a >> c >> p >> ms && k == key && (a == 4 || a == 8) && c >= 1 && p >= 0 && p <= 2) {
             *by = a; *kc = c; *pers = p;
             found = true;  // the last entry for a key wins
         }
@@ -523,6 +573,9 @@ extern "C" cps_status cps_batch_destroy(cps_batch *b)
     free_tables(b);
     for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
     if (b->done) cudaEventDestroy(b->done);
+    for (cudaStream_t st : b->side) cudaStreamDestroy(st);
+    for (cudaEvent_t e : b->side_done) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return CPS_OK;
@@ -575,7 +628,7 @@ extern "C" cps_status cps_batch_set_tile(cps_batch *b, int32_t rows, int32_t pla
     REQUIRE(b, CPS_E_INVALID, "cps_batch_set_tile: NULL batch");
     REQUIRE(rows == 4 || rows == 8, CPS_E_INVALID, "cps_batch_set_tile: rows must be 4 or 8");
     REQUIRE(planes >= 1 && planes <= 4096, CPS_E_INVALID, "cps_batch_set_tile: planes out of range");
-    REQUIRE(persistent == 0 || persistent == 1, CPS_E_INVALID, "cps_batch_set_tile: persistent is 0 or 1");
+    REQUIRE(persistent >= 0 && persistent <= 2, CPS_E_INVALID, "cps_batch_set_tile: persistent is 0, 1 or 2");
     if (b->by != rows || b->kc != planes || b->persistent != persistent) {
         b->by = rows; b->kc = planes; b->persistent = persistent;
         b->dirty = true;
@@ -655,7 +708,7 @@ extern "C" cps_status cps_batch_autotune(cps_batch *b, const char *cache_path, i
     const std::string key = bucket_key(b);
     int by, kc, pers;
     if (cache_lookup(cache_path, key, &by, &kc, &pers)) return cps_batch_set_tile(b, by, kc, pers);
-    static const int rows[] = {4, 8}, planes[] = {8, 16, 32, 64}, perss[] = {0, 1};
+    static const int rows[] = {4, 8}, planes[] = {8, 16, 32, 64}, perss[] = {0, 1, 2};
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

@@ -36,6 +36,20 @@ __device__ __forceinline__ void acquire_maps(const TmaMaps &M, bool eside)
     tensormap_acquire(&M.id);
 }
 
+// The views of a tile's grid are copied into shared memory when a block
+// moves to another grid: the sweep bodies then read pointers and CPML
+// coefficients with shared loads that no global field store can alias,
+// instead of reloading them from the descriptor table after every store.
+template <typename V>
+__device__ __forceinline__ void stage_view(V &dst, const V &src)
+{
+    static_assert(sizeof(V) % 8 == 0, "views are whole 8-byte words");
+    const int n = (int)(sizeof(V) / 8), nt = (int)(blockDim.x * blockDim.y);
+    const uint64_t *s = reinterpret_cast<const uint64_t *>(&src);
+    uint64_t *d = reinterpret_cast<uint64_t *>(&dst);
+    for (int w = (int)(threadIdx.y * blockDim.x + threadIdx.x); w < n; w += nt) d[w] = s[w];
+}
+
 template <typename T, int BY, bool PML>
 __global__ void __launch_bounds__(32 * BY) k_h_batch(const BatchGrid<T> *__restrict__ grids,
                                                       const int4 *__restrict__ tiles, int ntiles, int *err)
@@ -45,16 +59,22 @@ __global__ void __launch_bounds__(32 * BY) k_h_batch(const BatchGrid<T> *__restr
     unsigned char *sm = align_smem(sm_raw);
     init_stages(full);
     const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+    __shared__ FieldView<T> sf;
+    __shared__ PmlView<T> sp;
     uint32_t ctr = 0;
     int last = -1;
     for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
         const int4 e = tiles[q];
         const BatchGrid<T> &B = grids[e.x];
-        if (e.x != last) {
+        if (e.x != last) {  // uniform over the block: every thread reads the same entry
+            __syncthreads();  // the previous grid's views are no longer read
+            stage_view(sf, B.f);
+            if (PML) stage_view(sp, B.p);
             if (lead) acquire_maps(B.M, false);
+            __syncthreads();
             last = e.x;
         }
-        if (!h_tma_body<T, BY, PML>(B.M, B.f, B.p, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm, full)) return;
+        if (!h_tma_body<T, BY, PML>(B.M, sf, sp, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm, full)) return;
     }
 }
 
@@ -67,16 +87,26 @@ __global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restr
     unsigned char *sm = align_smem(sm_raw);
     init_stages(full);
     const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+    __shared__ FieldView<T> sf;
+    __shared__ PmlView<T> sp;
+    __shared__ DlView<T> sD;
+    __shared__ GainView<T> sG;
     uint32_t ctr = 0;
     int last = -1;
     for (int q = blockIdx.x; q < ntiles; q += gridDim.x) {
         const int4 e = tiles[q];
         const BatchGrid<T> &B = grids[e.x];
-        if (e.x != last) {
+        if (e.x != last) {  // uniform over the block
+            __syncthreads();
+            stage_view(sf, B.f);
+            if (PML) stage_view(sp, B.p);
+            if (DL) stage_view(sD, B.D);
+            if (GAIN) stage_view(sG, B.G);
             if (lead) acquire_maps(B.M, true);
+            __syncthreads();
             last = e.x;
         }
-        if (!e_tma_body<T, BY, PML, DL, GAIN>(B.M, B.f, B.p, B.D, B.G, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm,
+        if (!e_tma_body<T, BY, PML, DL, GAIN>(B.M, sf, sp, sD, sG, B.kc, TileXYZ{e.y, e.z, e.w}, ctr, err, sm,
                                                full))
             return;
     }

@@ -406,8 +406,11 @@ CPS_API cps_status cps_batch_info(const cps_batch *b, int32_t *ngrids, int64_t *
 CPS_API cps_status cps_batch_step(cps_batch *b, int32_t nsteps);
 /* wait for the batch stream; reports a device-side wait that gave up */
 CPS_API cps_status cps_batch_synchronize(cps_batch *b);
-/* tile rows (4 or 8), planes per tile, persistent launch (0: one block per
- * tile, 1: as many blocks as fit on the device, each walking the table) */
+/* tile rows (4 or 8), planes per tile, sweep launch mode (0: one launch per
+ * sweep class over all members' tiles, one block per tile; 1: the same with as
+ * many blocks as fit on the device, each walking the table; 2: every member's
+ * sweeps as its own one-grid launches, members spread over side streams so
+ * that several run at once).  Results do not depend on the choice. */
 CPS_API cps_status cps_batch_set_tile(cps_batch *b, int32_t rows, int32_t planes, int32_t persistent);
 CPS_API cps_status cps_batch_get_tile(const cps_batch *b, int32_t *rows, int32_t *planes, int32_t *persistent);
 /* CUDA-graph replay of step chunks (default on) */

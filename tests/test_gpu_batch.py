@@ -57,7 +57,8 @@ def _same(a, b, what=""):
         assert np.array_equal(x, y), f"{what} port sample"
 
 
-@pytest.mark.parametrize("tile", [(4, 8, 0, True), (8, 16, 1, True), (4, 32, 1, False), (8, 8, 0, False)])
+@pytest.mark.parametrize("tile", [(4, 8, 0, True), (8, 16, 1, True), (4, 32, 1, False), (8, 8, 0, False),
+                                  (4, 8, 2, True), (8, 64, 2, False)])
 def test_batch_equals_alone(tile):
     import cpsfdtd_b200 as cps
     steps = 70  # alone, port rings fold at 64 samples; in the batch, at every chunk
@@ -137,6 +138,8 @@ def test_batch_rejects_bad_members():
         b.add(g)
     with pytest.raises(cps.CpsError):
         b.set_tile(5, 8, 0)
+    with pytest.raises(cps.CpsError):
+        b.set_tile(4, 8, 3)
 
 
 def test_batch_autotune_cache(tmp_path):
@@ -148,7 +151,7 @@ def test_batch_autotune_cache(tmp_path):
         b.add(g)
     cache = str(tmp_path / "tune.txt")
     ran = b.autotune(cache, trial_steps=2)
-    assert ran == 16 * 3
+    assert ran == 24 * 3  # rows {4, 8} x planes {8, 16, 32, 64} x launch modes {0, 1, 2}, 1 + 2 steps each
     key = b.tune_key()
     lines = open(cache).read().splitlines()
     assert len(lines) == 1 and lines[0].split()[0] == key
