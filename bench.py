@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving leg (0: skip)")
     ap.add_argument("--serve-step-scale", type=float, default=2.0,
                     help="job step counts are the log-uniform [500, 20000] draws divided by this")
+    ap.add_argument("--serve-tile", default="",
+                    help="batch tile of the serving loop as rows,planes,mode (empty: the library default)")
     ap.add_argument("--serve-load", type=float, default=2.0,
                     help="offered load: arrival rate x job work / 20 Gcell-upd/s")
     return ap.parse_args()
@@ -387,7 +389,8 @@ def serving(args, local):
     budget = 180 * 10 ** 9
     free, total = torch.cuda.mem_get_info(local)
     budget = min(budget, int(free * 0.9))
-    srv = cps.Server(cps.FP32, max_jobs=256, budget_bytes=budget, chunk_steps=64)
+    tile = tuple(int(v) for v in args.serve_tile.split(",")) if args.serve_tile else None
+    srv = cps.Server(cps.FP32, max_jobs=256, budget_bytes=budget, chunk_steps=64, tile=tile)
     done = {}
     t0 = time.perf_counter()
     nxt = 0
@@ -445,7 +448,7 @@ def serving(args, local):
             "server_latency_p50_ms": st["latency_p50_ms"], "server_latency_p99_ms": st["latency_p99_ms"],
             "wait_p50_ms": st["wait_p50_ms"], "chunks": st["chunks"], "failed": st["jobs_failed"],
             "gpu_busy_s": st["gpu_busy_s"],
-            "budget_bytes": budget, "span_s": span,
+            "budget_bytes": budget, "span_s": span, "batch_tile": args.serve_tile or "library default (4,16,2)",
             "plain_one_at_a_time": {"jobs_per_s": len(jobs) / max(finish, 1e-9),
                                     "gcell_upd_per_s": cells_total / sum(service) / 1e9,
                                     "latency_p50_s": pct(plain_lat, 50), "latency_p99_s": pct(plain_lat, 99)},

@@ -86,7 +86,7 @@ struct cps_batch {
     std::vector<GridSig> sigs;
     bool dirty = true;
     // configuration
-    int by = 4, kc = 8, persistent = 0, graph = 1;
+    int by = 4, kc = 16, persistent = 2, graph = 1;  // per-member launches: fastest on the measured mixes
     // device tables (owned)
     std::vector<void *> owned;
     void *d_grids = nullptr;

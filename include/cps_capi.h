@@ -410,7 +410,8 @@ CPS_API cps_status cps_batch_synchronize(cps_batch *b);
  * sweep class over all members' tiles, one block per tile; 1: the same with as
  * many blocks as fit on the device, each walking the table; 2: every member's
  * sweeps as its own one-grid launches, members spread over side streams so
- * that several run at once).  Results do not depend on the choice. */
+ * that several run at once; the default, with 4 rows and 16 planes).  Results
+ * do not depend on the choice. */
 CPS_API cps_status cps_batch_set_tile(cps_batch *b, int32_t rows, int32_t planes, int32_t persistent);
 CPS_API cps_status cps_batch_get_tile(const cps_batch *b, int32_t *rows, int32_t *planes, int32_t *persistent);
 /* CUDA-graph replay of step chunks (default on) */
