@@ -307,8 +307,8 @@ cps_status rebuild_T(cps_batch *b)
                 dl.push_back(make_int4((int)gi, (int)c0, (int)std::min<int64_t>(c0 + 128, B.D.ncell), 0));
         }
         for (int side = 0; side < 2; ++side)
-            for (int t0 = 0; t0 < B.ntg[side]; t0 += 128)
-                inj[side].push_back(make_int4((int)gi, t0, std::min(t0 + 128, B.ntg[side]), 0));
+            for (int t0 = 0; t0 < B.ntg[side]; t0 += kInjPerBlock)
+                inj[side].push_back(make_int4((int)gi, t0, std::min(t0 + kInjPerBlock, B.ntg[side]), 0));
         for (int q = 0; q < B.nsrc; ++q) src.push_back(make_int2((int)gi, q));
         for (PortState &P : g->ports) {
             BatchPort<T> bp;
@@ -412,7 +412,7 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         });
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);
-        launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, st);
+        launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, S - 1, st);
         for (int c = 0; c < kNumSweep; ++c) n += b->ntiles[c] > 0;
         n += (b->ndl > 0) + (b->ninj[0] > 0) + (b->ninj[1] > 0) + (b->nsrc > 0) + (b->ngather > 0);
         for (int gi : b->big) n += 2 + (b->grids[gi]->dl_on && b->grids[gi]->dl_n > 0);

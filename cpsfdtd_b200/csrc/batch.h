@@ -52,6 +52,8 @@ struct BatchPort {
 };
 
 constexpr int kMaxRing = 64;  // samples per port ring = longest chunk
+constexpr int kInjThreads = 128;                // threads of a batched injection block
+constexpr int kInjPerBlock = 2 * kInjThreads;   // TF/SF targets per injection block entry
 
 // Work tables (device arrays):
 //   tiles      int4 {grid, bx, by, bz}      sweeps
@@ -79,7 +81,7 @@ template <typename T>
 void launch_sources_batch(const BatchGrid<T> *grids, const int2 *ents, int n, int step_off, cudaStream_t s);
 template <typename T>
 void launch_gather_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *blocks, int nblocks,
-                         int step_off, cudaStream_t s);
+                         int step_off, int last_off, cudaStream_t s);
 template <typename T>
 void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
                       const int4 *blocks, int nblocks, int nslots, cudaStream_t s);

@@ -120,6 +120,21 @@ struct FieldView {
     StretchView<T> s;
 };
 
+// a field component's array by index (Ex Ey Ez Hx Hy Hz), without an indexed
+// local array of pointers
+template <typename T>
+__host__ __device__ __forceinline__ T *field_comp(const FieldView<T> &f, int c)
+{
+    switch (c) {
+    case 0: return f.Ex;
+    case 1: return f.Ey;
+    case 2: return f.Ez;
+    case 3: return f.Hx;
+    case 4: return f.Hy;
+    default: return f.Hz;
+    }
+}
+
 template <typename T>
 struct DlView {
     int on;

@@ -215,18 +215,24 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
 // F += coef * inc(n - delay) * profile (TF_SF.cpp:992-1087, 1206-1299)
 // one TF/SF target: its contributions in the reference's face order
 template <typename T>
+__device__ __forceinline__ T inject_add(T v, const InjContrib &a, const T *table, int Nt, double n)
+{
+    const T inc = (T)inc_lookup<T>(table, Nt, n - a.delay);
+    return v + (T)a.coef * inc * (T)a.profile;
+}
+
+template <typename T>
 __device__ __forceinline__ void inject_target(const FieldView<T> &f, const InjTarget &q, const InjContrib *ct,
                                               const T *table, int Nt, double n, uint32_t face_mask)
 {
-    T *F[6] = {f.Ex, f.Ey, f.Ez, f.Hx, f.Hy, f.Hz};
-    T v = F[q.comp][q.idx];
+    T *F = field_comp(f, q.comp) + q.idx;
+    T v = *F;
     for (int c = q.start; c < q.start + q.count; ++c) {
         const InjContrib a = ct[c];
         if (!(face_mask & (1u << a.face))) continue;
-        const T inc = (T)inc_lookup<T>(table, Nt, n - a.delay);
-        v = v + (T)a.coef * inc * (T)a.profile;
+        v = inject_add(v, a, table, Nt, n);
     }
-    F[q.comp][q.idx] = v;
+    *F = v;
 }
 
 template <typename T>
@@ -238,16 +244,43 @@ __global__ void k_inject(FieldView<T> f, const InjTarget *tg, int ntarget, const
     inject_target<T>(f, tg[t], ct, table, Nt, n, face_mask);
 }
 
-// batched forms: the step number is the grid's chunk start plus step_off
+// batched forms: the step number is the grid's chunk start plus step_off.
+// A block entry covers kInjPerBlock targets; each thread takes two of them,
+// kInjThreads apart, and requests both targets' records, field values and
+// first contributions before using any (the kernel is bound by the latency
+// of these dependent loads).  Each target's contributions are added in its
+// own order, as in inject_target; the two targets are distinct (cell,
+// component) pairs, so their updates are independent.
 template <typename T>
-__global__ void k_inject_batch(const BatchGrid<T> *__restrict__ grids, const int4 *__restrict__ blocks, int side,
-                               int step_off)
+__global__ void __launch_bounds__(kInjThreads) k_inject_batch(const BatchGrid<T> *__restrict__ grids,
+                                                              const int4 *__restrict__ blocks, int side,
+                                                              int step_off)
 {
     const int4 e = blocks[blockIdx.x];
-    const int t = e.y + (int)threadIdx.x;
-    if (t >= e.z) return;
+    const int t0 = e.y + (int)threadIdx.x, t1 = t0 + kInjThreads;
+    if (t0 >= e.z) return;
+    const bool two = t1 < e.z;
     const BatchGrid<T> &B = grids[e.x];
-    inject_target<T>(B.f, B.tg[side][t], B.ct[side], B.inc[side], B.Nt, (double)(B.n0 + step_off), CPS_FACE_ALL);
+    const InjTarget *tg = B.tg[side];
+    const InjContrib *ct = B.ct[side];
+    const T *table = B.inc[side];
+    const int Nt = B.Nt;
+    const double n = (double)(B.n0 + step_off);
+    const InjTarget q0 = tg[t0];
+    const InjTarget q1 = two ? tg[t1] : q0;
+    T *F0 = field_comp(B.f, q0.comp) + q0.idx;
+    T *F1 = field_comp(B.f, q1.comp) + q1.idx;
+    T v0 = *F0;
+    T v1 = two ? *F1 : T(0);
+    const InjContrib a0 = ct[q0.start];  // every target has at least one contribution
+    const InjContrib a1 = ct[q1.start];
+    v0 = inject_add(v0, a0, table, Nt, n);
+    for (int c = q0.start + 1; c < q0.start + q0.count; ++c) v0 = inject_add(v0, ct[c], table, Nt, n);
+    *F0 = v0;
+    if (!two) return;
+    v1 = inject_add(v1, a1, table, Nt, n);
+    for (int c = q1.start + 1; c < q1.start + q1.count; ++c) v1 = inject_add(v1, ct[c], table, Nt, n);
+    *F1 = v1;
 }
 
 template <typename T>
@@ -366,7 +399,7 @@ void launch_inject_batch(const BatchGrid<T> *grids, const int4 *blocks, int nblo
                          cudaStream_t s)
 {
     if (nblocks <= 0) return;
-    k_inject_batch<T><<<nblocks, 128, 0, s>>>(grids, blocks, side, step_off);
+    k_inject_batch<T><<<nblocks, kInjThreads, 0, s>>>(grids, blocks, side, step_off);
 }
 
 template <typename T>

@@ -138,24 +138,42 @@ __global__ void __launch_bounds__(256, 2) k_dft(const T *ring, int npts, int nsl
 }
 
 // batched forms over the ports of many grids
+// A chunk's rings are read only by its DFT contraction (the components the
+// port transforms) and by the last-sample read-out (the slot of the chunk's
+// last step, all six components).  So the last step (last_off) samples all
+// six components, earlier steps only the transformed ones, and a port without
+// a DFT (one slot, overwritten every step) only the last step.
 template <typename T>
 __global__ void k_gather_batch(const BatchGrid<T> *__restrict__ grids, const BatchPort<T> *__restrict__ ports,
-                               const int2 *__restrict__ blocks, int step_off)
+                               const int2 *__restrict__ blocks, int step_off, int last_off)
 {
     const int2 e = blocks[blockIdx.x];
     const BatchPort<T> &P = ports[e.x];
+    const bool last = step_off == last_off;
+    if (!last && P.slots == 1) return;
     const int p = e.y + (int)threadIdx.x;
     const int npts = P.npts;
     if (p >= npts) return;
     const FieldView<T> &f = grids[P.grid].f;
     T *slot = P.ring + (int64_t)(P.slots == 1 ? 0 : step_off) * 6 * npts;
     const int64_t g = P.idx[p];
-    slot[p] = f.Ex[g];
-    slot[npts + p] = f.Ey[g];
-    slot[2 * (int64_t)npts + p] = f.Ez[g];
-    slot[3 * (int64_t)npts + p] = f.Hx[g];
-    slot[4 * (int64_t)npts + p] = f.Hy[g];
-    slot[5 * (int64_t)npts + p] = f.Hz[g];
+    if (last) {
+        slot[p] = f.Ex[g];
+        slot[npts + p] = f.Ey[g];
+        slot[2 * (int64_t)npts + p] = f.Ez[g];
+        slot[3 * (int64_t)npts + p] = f.Hx[g];
+        slot[4 * (int64_t)npts + p] = f.Hy[g];
+        slot[5 * (int64_t)npts + p] = f.Hz[g];
+        return;
+    }
+    const int nc = P.ncomp;
+    T v[6];
+#pragma unroll
+    for (int ci = 0; ci < 6; ++ci)  // every load before the first store
+        if (ci < nc) v[ci] = field_comp(f, __ldg(&P.comps[ci]))[g];
+#pragma unroll
+    for (int ci = 0; ci < 6; ++ci)
+        if (ci < nc) slot[(int64_t)__ldg(&P.comps[ci]) * npts + p] = v[ci];
 }
 
 template <typename T>
@@ -270,10 +288,10 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
 
 template <typename T>
 void launch_gather_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *blocks, int nblocks,
-                         int step_off, cudaStream_t s)
+                         int step_off, int last_off, cudaStream_t s)
 {
     if (nblocks <= 0) return;
-    k_gather_batch<T><<<nblocks, 256, 0, s>>>(grids, ports, blocks, step_off);
+    k_gather_batch<T><<<nblocks, 256, 0, s>>>(grids, ports, blocks, step_off, last_off);
 }
 
 template <typename T>
@@ -332,7 +350,7 @@ void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s
     template void launch_to_device_layout<T>(const double *, T *, Dims, cudaStream_t);                     \
     template void launch_from_device_layout<T>(const T *, double *, Dims, cudaStream_t);                   \
     template void launch_gather_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int, int, \
-                                         cudaStream_t);                                                    \
+                                         int, cudaStream_t);                                               \
     template void launch_dft_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int,       \
                                       const int4 *, int, int, cudaStream_t);                             \
     template void dft_batch_attributes<T>();
