@@ -528,9 +528,11 @@ class Grid:
 
 class Batch:
     """Many grids of one precision advanced together by the batched engine
-    (``cps_batch_*``): one launch per sweep class over all members' tiles,
-    step chunks replayed as CUDA graphs.  Members stay ordinary
-    :class:`Grid` objects for set-up and read-out."""
+    (``cps_batch_*``): sweeps either as one launch per sweep class over all
+    members' tiles or as each member's own launches spread over side streams
+    (the default), the rest of a step batched over members, step chunks
+    replayed as CUDA graphs.  Members stay ordinary :class:`Grid` objects for
+    set-up and read-out."""
 
     def __init__(self, precision=FP32):
         self.L = lib()
@@ -569,6 +571,10 @@ class Batch:
         _check(self.L.cps_batch_synchronize(self.h))
 
     def set_tile(self, rows, planes, persistent=0):
+        """Tile rows (4 or 8), planes per tile and sweep launch mode: 0 one
+        launch per sweep class, one block per tile; 1 the same, persistent;
+        2 each member's own launches on side streams (the default, with
+        4 rows and 16 planes).  Results do not depend on the choice."""
         _check(self.L.cps_batch_set_tile(self.h, rows, planes, persistent))
 
     def get_tile(self):
