@@ -105,11 +105,15 @@ def test_batch_membership_changes_and_interleaved_alone_steps():
     _same(ref_c, _state(gc), "c")
 
 
-def test_batch_fp64_equals_alone_and_oracle(oracle_mod):
+@pytest.mark.parametrize("tile", [(4, 16, 2), (4, 8, 0)])
+def test_batch_fp64_equals_alone_and_oracle(oracle_mod, tile):
+    """FP64 through both sweep forms: the member's own launches (the default)
+    and the class launches over the shared tile table."""
     import cpsfdtd_b200 as cps
     dk = decks.config2(n=36, steps=50, nfreq=2)
     ref = _alone(dk, cps.FP64, 50)
     b = cps.Batch(cps.FP64)
+    b.set_tile(*tile)
     g = _grid(dk, cps.FP64)
     b.add(g)
     b.step(50)

@@ -25,9 +25,9 @@ def _result(g):
     return out
 
 
-def _serve(cps, jobs, arrivals, chunk=64, budget=8 * 10 ** 9, max_jobs=16, polls_between=1):
+def _serve(cps, jobs, arrivals, chunk=64, budget=8 * 10 ** 9, max_jobs=16, polls_between=1, tile=None):
     """Submit job n after arrivals[n] polls; returns {index: (status, result)}."""
-    srv = cps.Server(cps.FP32, max_jobs=max_jobs, budget_bytes=budget, chunk_steps=chunk)
+    srv = cps.Server(cps.FP32, max_jobs=max_jobs, budget_bytes=budget, chunk_steps=chunk, tile=tile)
     res = {}
     order = sorted(range(len(jobs)), key=lambda n: arrivals[n])
     polls = 0
@@ -58,16 +58,19 @@ def _same(a, b):
         assert np.array_equal(x, y)
 
 
-def test_alone_equals_mix():
+@pytest.mark.parametrize("tile", [None, (4, 8, 0)])
+def test_alone_equals_mix(tile):
+    """Default batch tiling (each member's own sweep launches) and the class
+    launches over a shared tile table give the same per-job results."""
     import cpsfdtd_b200 as cps
     jobs = _job_decks()
     alone = {}
     for n, job in enumerate(jobs):
-        r, st = _serve(cps, [job], [0])
+        r, st = _serve(cps, [job], [0], tile=tile)
         assert r[0][0] == 0 and st["jobs_done"] == 1
         alone[n] = r[0][1]
     # the same jobs arriving while others run, with a chunk that splits them
-    mix, st = _serve(cps, jobs, [0, 1, 3, 4], chunk=24)
+    mix, st = _serve(cps, jobs, [0, 1, 3, 4], chunk=24, tile=tile)
     assert st["jobs_done"] == len(jobs) and st["jobs_failed"] == 0
     assert st["latency_p99_ms"] >= st["latency_p50_ms"] > 0
     for n in range(len(jobs)):
