@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "grid.h"
+#include "tfsf_csr.h"
 
 namespace cps {
 
@@ -1280,77 +1281,11 @@ extern "C" cps_status cps_tfsf_init(cps_grid *g, const cps_tfsf_params *p)
                 }
             }
         });
-        // targets in device order, so neighbouring threads touch neighbouring cells;
-        // a stable sort by key keeps each target's contributions in the reference's
-        // face order.  Items are placed by plane exactly as a serial counting sort
-        // over the strips in face order would place them (strip by strip, each
-        // strip's items in order), then stable-sorted within each plane; the
-        // counting, the scatter, the sorts and the target runs each run on the
-        // host threads, per strip or per plane.
-        const int nz1 = d.nz + 1;
-        const int ns = (int)strips.size();
-        auto plane_of = [&](const Item &it) { return (size_t)(it.key / 8 / d.pxy); };
-        std::vector<std::vector<size_t>> off(ns, std::vector<size_t>(nz1, 0));  // counts, then first slots
-        parallel_for(ns, [&](int s0, int s1) {
-            for (int st = s0; st < s1; ++st)
-                for (const Item &it : strips[st]) off[st][plane_of(it)]++;
-        });
-        std::vector<size_t> start(nz1 + 1, 0);
-        for (int k = 0; k < nz1; ++k) {
-            size_t at = start[k];
-            for (int st = 0; st < ns; ++st) {
-                const size_t c = off[st][k];
-                off[st][k] = at;
-                at += c;
-            }
-            start[k + 1] = at;
-        }
-        std::vector<Item> items(start[nz1]);
-        parallel_for(ns, [&](int s0, int s1) {
-            for (int st = s0; st < s1; ++st) {
-                std::vector<size_t> &o = off[st];
-                for (const Item &it : strips[st]) items[o[plane_of(it)]++] = it;
-            }
-        });
-        strips.clear();
-        parallel_for(nz1, [&](int k0, int k1) {
-            for (int k = k0; k < k1; ++k)
-                std::stable_sort(items.begin() + start[k], items.begin() + start[k + 1],
-                                 [](const Item &a, const Item &b) { return a.key < b.key; });
-        });
-        // one target per run of equal keys (a run never crosses a plane); the
-        // contributions keep the item order, so a target's run starts at its
-        // first item
-        std::vector<size_t> tg_at(nz1 + 1, 0);
-        parallel_for(nz1, [&](int k0, int k1) {
-            for (int k = k0; k < k1; ++k) {
-                size_t n = 0;
-                for (size_t q = start[k]; q < start[k + 1]; ++q) n += q == start[k] || items[q].key != items[q - 1].key;
-                tg_at[k + 1] = n;
-            }
-        });
-        for (int k = 0; k < nz1; ++k) tg_at[k + 1] += tg_at[k];
-        std::vector<InjTarget> tg(tg_at[nz1]);
-        std::vector<InjContrib> ct(items.size());
-        parallel_for(nz1, [&](int k0, int k1) {
-            for (int k = k0; k < k1; ++k) {
-                size_t t = tg_at[k];
-                for (size_t q = start[k]; q < start[k + 1];) {
-                    size_t r = q;
-                    while (r < start[k + 1] && items[r].key == items[q].key) {
-                        ct[r] = items[r].c;
-                        ++r;
-                    }
-                    InjTarget &tt = tg[t++];
-                    tt.idx = items[q].key / 8;
-                    tt.comp = (int)(items[q].key % 8);
-                    tt.start = (int32_t)q;
-                    tt.count = (int32_t)(r - q);
-                    tt.face = items[q].c.face;
-                    q = r;
-                }
-            }
-        });
+        // targets in device order, so neighbouring threads touch neighbouring
+        // cells, each with its contributions in the reference's face order
+        std::vector<InjTarget> tg;
+        std::vector<InjContrib> ct;
+        tfsf_assemble(strips, d.nz + 1, d.pxy, [](int n, auto f) { parallel_for(n, f); }, tg, ct);
         const int side = isH;  // d_tg[0] = E targets, d_tg[1] = H targets
         g->ntg[side] = (int)tg.size();
         if ((s = dalloc(g, (void **)&g->d_tg[side], tg.size() * sizeof(InjTarget)))) return s;
