@@ -89,7 +89,7 @@ void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, cons
 template <typename T>
 void batch_kernel_attributes();
 template <typename T>
-void dft_batch_attributes();
+bool dft_batch_attributes();
 // sweep blocks of one SM that fit at once (for persistent launches)
 template <typename T>
 int batch_blocks_per_sm(int by, bool eside, int cls);

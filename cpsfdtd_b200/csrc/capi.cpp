@@ -350,6 +350,9 @@ cps_status flush_dft_T(cps_grid *g, PortState &P)
     }
     launch_port_dft<T>((const T *)P.d_ring, P.npts, P.fill, P.ring_n0, g->desc.dt, P.d_omega, P.nfreq, P.d_comps,
                        P.ncomp, P.d_acc, g->d_phasor, g->stream);
+    // a failed launch leaves the ring as it was, so a later flush folds its samples
+    const cudaError_t e = cudaGetLastError();
+    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("port DFT launch failed: ") + cudaGetErrorString(e));
     g->launches += 2;
     // keep the last sample readable: move it to slot 0
     if (P.last_slot > 0) {
@@ -1410,6 +1413,7 @@ extern "C" cps_status cps_port_set_dft(cps_grid *g, int32_t port_id, int32_t nfr
     if ((s = dalloc(g, (void **)&P.d_comps, 6 * sizeof(int32_t)))) return s;
     if ((s = upload_raw(g, P.d_comps, P.comps, 6 * sizeof(int32_t)))) return s;
     if ((s = dalloc(g, (void **)&P.d_acc, (size_t)P.ncomp * nfreq * 2 * P.npts * sizeof(double)))) return s;
+    if ((s = dalloc(g, (void **)&P.d_flux, nfreq * sizeof(double)))) return s;
     // a ring of 64 samples between contractions
     dfree(g, P.d_ring);
     P.slots = 64;
@@ -1480,13 +1484,13 @@ extern "C" cps_status cps_port_flux(cps_grid *g, int32_t port_id, char normal, d
     }
     cps_status s = flush_dft(g, P);
     if (s) return s;
-    double *d_out = nullptr;
-    if ((s = dalloc(g, (void **)&d_out, P.nfreq * sizeof(double)))) return s;
-    launch_port_flux(P.d_acc, P.npts, P.nfreq, P.ncomp, sel, dA, d_out, g->stream);
+    // the port's own result buffer, allocated with its accumulators
+    launch_port_flux(P.d_acc, P.npts, P.nfreq, P.ncomp, sel, dA, P.d_flux, g->stream);
+    const cudaError_t e0 = cudaGetLastError();
+    REQUIRE(e0 == cudaSuccess, CPS_E_CUDA, std::string("cps_port_flux: launch failed: ") + cudaGetErrorString(e0));
     g->launches++;
-    cudaError_t e1 = cudaMemcpyAsync(out, d_out, P.nfreq * sizeof(double), cudaMemcpyDeviceToHost, g->stream);
+    cudaError_t e1 = cudaMemcpyAsync(out, P.d_flux, P.nfreq * sizeof(double), cudaMemcpyDeviceToHost, g->stream);
     cudaError_t e2 = cudaStreamSynchronize(g->stream);
-    dfree(g, d_out);
     REQUIRE(e1 == cudaSuccess && e2 == cudaSuccess, CPS_E_CUDA, "cps_port_flux: copy failed");
     return CPS_OK;
 }

@@ -14,10 +14,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
 #include "../../include/cps_capi.h"
+#include "attr_once.h"
 
 namespace cps {
 
@@ -172,6 +174,31 @@ struct ThreeView {
     double *state;        // [word][ncell]
     ThreeCoef c;
 };
+
+// Dynamic shared memory of kernel `func` (and, carveout >= 0, its preferred
+// shared-memory carveout), set once per device through `done` (one flag word
+// per kernel).  Returns the attribute call's error; the runtime also keeps it
+// as the thread's last error, so the launch check that follows reports it.
+inline cudaError_t smem_attr_once(std::atomic<uint64_t> &done, const void *func, int bytes, int carveout = -1)
+{
+    return (cudaError_t)attr_once_per_device(
+        done, [](int *dev) { return (int)cudaGetDevice(dev); },
+        [&]() {
+            cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e == cudaSuccess && carveout >= 0)
+                e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, carveout);
+            return (int)e;
+        });
+}
+
+// the same for a kernel given as a template argument, one flag per kernel;
+// true when the kernel may be launched
+template <auto K>
+bool kernel_smem(int bytes, int carveout = -1)
+{
+    static std::atomic<uint64_t> done{0};
+    return smem_attr_once(done, reinterpret_cast<const void *>(K), bytes, carveout) == cudaSuccess;
+}
 
 // ------------------------------------------------------------ launchers
 // Plain path: one kernel per reference routine (kernels_plain.cu, built

@@ -45,6 +45,7 @@ struct PortState {
     int32_t *d_comps = nullptr;
     double *d_omega = nullptr;
     double *d_acc = nullptr;  // [ncomp][nfreq][2][npts]
+    double *d_flux = nullptr; // [nfreq]: cps_port_flux's result, allocated with the accumulators
 };
 
 // one recorded per-routine call (cps_op_*), kept until the recorder flushes

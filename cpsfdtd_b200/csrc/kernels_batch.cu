@@ -133,21 +133,18 @@ __global__ void k_advance(BatchGrid<T> *grids, int ngrids, int nsteps)
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// set once per kernel and device; false when the attribute could not be set
 template <auto K>
-void smem_attr(int bytes)
+bool smem_attr(int bytes)
 {
-    static bool done = false;  // one flag per kernel
-    if (!done) {
-        cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        done = true;
-    }
+    return kernel_smem<K>(bytes);
 }
 
 template <typename T, int BY, bool PML>
 void h_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    smem_attr<k_h_batch<T, BY, PML>>(L::SMEM);
+    if (!smem_attr<k_h_batch<T, BY, PML>>(L::SMEM)) return;
     k_h_batch<T, BY, PML><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
 }
 
@@ -155,8 +152,8 @@ template <typename K>
 int occupancy(K kernel, int threads, int smem)
 {
     int n = 0;
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
@@ -167,7 +164,7 @@ template <typename T, int BY, bool PML, bool GAIN, bool DL>
 void e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    smem_attr<k_e_batch<T, BY, PML, GAIN, DL>>(L::SMEM);
+    if (!smem_attr<k_e_batch<T, BY, PML, GAIN, DL>>(L::SMEM)) return;
     k_e_batch<T, BY, PML, GAIN, DL><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
 }
 

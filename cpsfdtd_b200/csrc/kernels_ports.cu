@@ -278,11 +278,7 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
     double2 *tab = reinterpret_cast<double2 *>(scratch_phasor);
     k_phasors<<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, tab);
     dim3 grid(cdiv(npts, kPT), ncomp, cdiv(nfreq, kFT));
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_dft<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem(sizeof(T)));
-        attr = true;
-    }
+    if (!kernel_smem<k_dft<T>>((int)kDftSmem(sizeof(T)))) return;
     k_dft<T><<<grid, 256, kDftSmem(sizeof(T)), s>>>(ring, npts, nslots, tab, nfreq, comps, acc);
 }
 
@@ -295,13 +291,9 @@ void launch_gather_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, c
 }
 
 template <typename T>
-void dft_batch_attributes()
+bool dft_batch_attributes()
 {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_dft_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmem(sizeof(T)));
-        attr = true;
-    }
+    return kernel_smem<k_dft_batch<T>>((int)kDftSmem(sizeof(T)));
 }
 
 template <typename T>
@@ -310,7 +302,7 @@ void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, cons
 {
     if (nph <= 0 || nblocks <= 0 || nslots <= 0) return;
     k_phasors_batch<T><<<nph, 256, 0, s>>>(grids, ports, ph_blocks, nslots);
-    dft_batch_attributes<T>();
+    if (!dft_batch_attributes<T>()) return;
     k_dft_batch<T><<<nblocks, 256, kDftSmem(sizeof(T)), s>>>(ports, blocks, nslots);
 }
 
@@ -353,7 +345,7 @@ void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s
                                          int, cudaStream_t);                                               \
     template void launch_dft_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int,       \
                                       const int4 *, int, int, cudaStream_t);                             \
-    template void dft_batch_attributes<T>();
+    template bool dft_batch_attributes<T>();
 CPS_INST(double)
 CPS_INST(float)
 

@@ -356,16 +356,12 @@ __global__ void __launch_bounds__(256) k_h_corrections(const InjContrib *__restr
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-// dynamic shared memory and the largest shared-memory carveout, set once per kernel
+// dynamic shared memory and the largest shared-memory carveout, set once per
+// kernel and device
 template <auto K>
-void set_smem(int bytes)
+bool set_smem(int bytes)
 {
-    static bool done = false;
-    if (!done) {
-        cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        cudaFuncSetAttribute(K, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        done = true;
-    }
+    return kernel_smem<K>(bytes, 100);
 }
 
 template <typename T, int BY, bool PML, bool DL, bool GAIN, bool TFSF>
@@ -374,7 +370,7 @@ void step_launch(const StepMaps &M, const FieldView<T> &fo, const FieldView<T> &
                  int *err, cudaStream_t s)
 {
     using L = StepLayout<T, BY>;
-    set_smem<k_step_tma<T, BY, PML, DL, GAIN, TFSF>>(L::SMEM);
+    if (!set_smem<k_step_tma<T, BY, PML, DL, GAIN, TFSF>>(L::SMEM)) return;
     const Dims &d = fo.d;
     dim3 grid(cdiv(d.nx + 1, 32), cdiv(d.ny + 1, BY), cdiv(d.nz, kc));
     k_step_tma<T, BY, PML, DL, GAIN, TFSF><<<grid, dim3(32, BY + 2), L::SMEM, s>>>(M, fo, fn, pin, pout, D, G, hc, kc,

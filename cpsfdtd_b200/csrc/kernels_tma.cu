@@ -56,16 +56,12 @@ __global__ void __launch_bounds__(128) k_dl_cells(FieldView<T> f, PmlView<T> p, 
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
-// the shared-memory attribute of each kernel, set once (outside any capture
-// when tma_attributes runs first)
+// the shared-memory attribute of each kernel, set once per device (outside
+// any capture when tma_attributes runs first)
 template <auto K>
-void set_smem(int bytes)
+bool set_smem(int bytes)
 {
-    static bool done = false;
-    if (!done) {
-        cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        done = true;
-    }
+    return kernel_smem<K>(bytes);
 }
 
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
@@ -73,7 +69,7 @@ void e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, 
                   const GainView<T> &G, int kc, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM);
+    if (!set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM)) return;
     dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
     k_e_tma<T, BY, PML, DL, GAIN><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, err);
 }
@@ -82,7 +78,7 @@ template <typename T, int BY, bool PML>
 void h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    set_smem<k_h_tma<T, BY, PML>>(L::SMEM);
+    if (!set_smem<k_h_tma<T, BY, PML>>(L::SMEM)) return;
     dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
     k_h_tma<T, BY, PML><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, err);
 }

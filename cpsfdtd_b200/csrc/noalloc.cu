@@ -64,6 +64,9 @@ cps_status flush_static_T(cps_grid *g, double *scratch)
         if (P.nfreq == 0 || P.fill == 0) continue;
         launch_port_dft<T>((const T *)P.d_ring, P.npts, P.fill, P.ring_n0, g->desc.dt, P.d_omega, P.nfreq, P.d_comps,
                            P.ncomp, P.d_acc, scratch, g->stream);
+        // a failed launch leaves the ring as it was, so a later flush folds its samples
+        const cudaError_t e = cudaGetLastError();
+        REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("cps_ports_flush_static: ") + cudaGetErrorString(e));
         g->launches += 2;
         // keep the last sample readable: move it to slot 0
         if (P.last_slot > 0) {
@@ -73,8 +76,6 @@ cps_status flush_static_T(cps_grid *g, double *scratch)
         }
         P.fill = 0;
     }
-    const cudaError_t e = cudaGetLastError();
-    REQUIRE(e == cudaSuccess, CPS_E_CUDA, std::string("cps_ports_flush_static: ") + cudaGetErrorString(e));
     return CPS_OK;
 }
 

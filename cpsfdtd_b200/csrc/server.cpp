@@ -24,6 +24,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -69,7 +70,7 @@ struct Job {
     cps_status build_status = CPS_OK;
     int64_t cells = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
-    volatile bool cancel = false;
+    std::atomic<bool> cancel{false};  // set by cps_server_cancel on the caller's thread, read by the poll and builder threads
 };
 
 double percentile(std::vector<double> v, double q)

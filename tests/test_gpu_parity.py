@@ -187,3 +187,42 @@ def test_three_level_rejects_a_second_gain_and_batches():
     with pytest.raises(cps.CpsError):
         b.add(g)
     b.close()
+
+
+# tangential pairs of the net Poynting flux along a port's normal:
+# S_n = Re(E_a conj(H_b) - E_c conj(H_e)) / 2
+FLUX_PAIRS = {"x": (1, 5, 2, 4), "y": (2, 3, 0, 5), "z": (0, 4, 1, 3)}
+
+
+def _oracle_flux(dft, mask, normal, dA):
+    """The flux from the oracle's FP64 port DFT ([npts][ncomp][nfreq][2])."""
+    comps = [c for c in range(6) if mask & (1 << c)]
+    a, b, c, e = (comps.index(x) for x in FLUX_PAIRS[normal])
+    z = dft[..., 0] + 1j * dft[..., 1]
+    s = (z[:, a] * np.conj(z[:, b]) - z[:, c] * np.conj(z[:, e])).real.sum(axis=0)
+    return 0.5 * s * dA
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32"])
+def test_port_flux_matches_oracle(prec, oracle_runs):
+    """cps_port_flux on the six planar ports of the dispersive deck against
+    the flux formed from the oracle's FP64 DFT of the same samples (the port
+    samples themselves follow Ports.cpp:201-353 and are pinned to the
+    reference's series); two calls in a row give the same result."""
+    import cpsfdtd_b200 as cps
+    dk, ids, pts, o = oracle_runs["c2"]
+    g = cps.Grid.from_deck(dk, prec, ids=ids, port_points_list=pts)
+    g.step(dk.nsteps, cps.FUSED)
+    # FP32: the flux is a product of two DFTs each within the 1e-4 bar
+    tol = FP64_TOL if prec == 0 else 2 * FP32_TOL
+    area = {"x": dk.dy * dk.dz, "y": dk.dx * dk.dz, "z": dk.dx * dk.dy}
+    for n, p in enumerate(dk.ports):
+        normal = p.params["dir"]
+        want = _oracle_flux(o.port_dft(n, bin(p.dft_mask).count("1"), len(p.dft_freqs)), p.dft_mask, normal,
+                            area[normal])
+        got = g.port_flux(n, normal)
+        assert np.abs(want).max() > 0
+        err = np.abs(got - want).max() / np.abs(want).max()
+        assert err <= tol, f"port {n} ({normal}) flux error {err:.3e}"
+        assert np.array_equal(g.port_flux(n, normal), got)
+    g.close()
