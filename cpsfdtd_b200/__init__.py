@@ -143,6 +143,7 @@ def lib():
             "cps_field_download": ([P, I32, dp], I32), "cps_field_upload": ([P, I32, dp], I32),
             "cps_field_download_f32": ([P, I32, C.POINTER(C.c_float)], I32),
             "cps_grid_reset": ([P, I64], I32), "cps_grid_check_finite": ([P, C.POINTER(I64)], I32),
+            "cps_grid_set_wait_skew": ([P, I32], I32),
             "cps_gain_populations": ([P, dp, C.POINTER(I64)], I32),
             "cps_grid_launch_count": ([P, C.POINTER(I64)], I32),
             "cps_ports_flush": ([P], I32), "cps_grid_set_timing": ([P, I32], I32),
@@ -407,6 +408,10 @@ class Grid:
 
     def reset(self, n0=1):
         _check(self.L.cps_grid_reset(self.h, n0))
+
+    def set_wait_skew(self, extra_bytes):
+        """Test setting of the bounded device waits (cps_grid_set_wait_skew)."""
+        _check(self.L.cps_grid_set_wait_skew(self.h, extra_bytes))
 
     def op(self, name, *args):
         _check(getattr(self.L, "cps_op_" + name)(self.h, *args))

@@ -344,8 +344,8 @@ cps_status rebuild_T(cps_batch *b)
     cps_status s;
     if ((s = upload_vec(b, (BatchGrid<T> **)&b->d_grids, hg))) return s;
     if ((s = upload_vec(b, (BatchPort<T> **)&b->d_ports, hp))) return s;
-    if ((s = bmalloc(b, (void **)&b->d_err, sizeof(int)))) return s;
-    CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
+    if ((s = bmalloc(b, (void **)&b->d_err, 2 * sizeof(int)))) return s;  // error code, wait test setting (0)
+    CK(cudaMemsetAsync(b->d_err, 0, 2 * sizeof(int), b->stream));
     // kernel attributes are set here, outside any stream capture
     batch_kernel_attributes<T>();
     tma_attributes<T>();
@@ -543,6 +543,14 @@ bool cache_lookup(const char *path, const std::string &key, int *by, int *kc, in
 }
 
 }  // namespace
+
+// clears a batch's device error word (the grid reset of a grid stepped
+// through its internal one-grid batch)
+cps_status cps::batch_clear_error(cps_batch *b)
+{
+    if (b->d_err) CK(cudaMemsetAsync(b->d_err, 0, sizeof(int), b->stream));
+    return CPS_OK;
+}
 
 // ================================================================ C ABI
 

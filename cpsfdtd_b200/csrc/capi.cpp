@@ -732,7 +732,7 @@ extern "C" cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out)
     if (!s) s = dalloc(g, (void **)&g->d_id, (size_t)g->elems);
     if (!s) s = dalloc(g, &g->d_media, 4 * 256 * g->esz);
     if (!s) s = dalloc(g, (void **)&g->d_counter, sizeof(unsigned long long));
-    if (!s) s = dalloc(g, (void **)&g->d_err, sizeof(int));
+    if (!s) s = dalloc(g, (void **)&g->d_err, 2 * sizeof(int));  // error code, wait test setting
     if (s) { cps_grid_destroy(g); return s; }
     g->ids_dev.assign((size_t)g->elems, 0);
     // stretched coordinates start at 1/delta (Structure.cpp:425-445)
@@ -1954,7 +1954,24 @@ extern "C" cps_status cps_grid_reset(cps_grid *g, int64_t n0)
         CK(cudaMemsetAsync(P.d_ring, 0, (size_t)P.slots * 6 * P.npts * g->esz, g->stream));
         if (P.d_acc) CK(cudaMemsetAsync(P.d_acc, 0, (size_t)P.ncomp * P.nfreq * 2 * P.npts * sizeof(double), g->stream));
     }
+    // a sweep that gave up left the state incomplete; the reset state is whole again
+    CK(cudaMemsetAsync(g->d_err, 0, sizeof(int), g->stream));
+    if (g->solo) {
+        cps_status s = batch_clear_error(g->solo);
+        if (s) return s;
+    }
     g->step = n0;
+    CK(cudaStreamSynchronize(g->stream));
+    return CPS_OK;
+}
+
+extern "C" cps_status cps_grid_set_wait_skew(cps_grid *g, int32_t extra_bytes)
+{
+    REQUIRE(g, CPS_E_INVALID, "NULL grid");
+    REQUIRE(extra_bytes >= 0 && extra_bytes <= 4096, CPS_E_INVALID, "cps_grid_set_wait_skew: 0..4096 bytes");
+    FLUSH_RECORDED(g);
+    CK(cudaSetDevice(g->desc.device));
+    CK(cudaMemcpyAsync(g->d_err + 1, &extra_bytes, sizeof(int), cudaMemcpyHostToDevice, g->stream));
     CK(cudaStreamSynchronize(g->stream));
     return CPS_OK;
 }

@@ -337,4 +337,7 @@ inline ThreeView three_view(const cps_grid *g)
     return v;
 }
 
+// clears the device error word of a batch (batch.cpp)
+cps_status batch_clear_error(cps_batch *b);
+
 }  // namespace cps

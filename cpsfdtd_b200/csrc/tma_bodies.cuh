@@ -20,8 +20,16 @@
 // through the ring, so a block may run several tiles in a row (persistent
 // launches): plane q of the block's life uses stage q % kStages and waits for
 // mbarrier phase parity (q / kStages) & 1.  The mbarriers are initialised once
-// per block by the caller (init_stages).  Every wait is bounded; on expiry the
-// body records an error code for the host and returns false.
+// per block by the caller (init_stages).
+//
+// Every wait is bounded (kWaitLimit polls and kWaitNs of wall-clock time,
+// whichever ends first).  When a wait gives up, the body records an error
+// code in err[0] for the host, thread 0 waits (bounded again) for the loads
+// of the other planes still in flight so that no copy into the block's shared
+// memory outlives it, and the body returns false.  err[1] is a test setting
+// (0 in normal use): the first plane of every tile then expects err[1] more
+// bytes than its loads bring, so its wait runs out and the sweep reports the
+// timeout without any fault (cps_grid_set_wait_skew).
 #pragma once
 
 #include "sweep_cells.cuh"
@@ -31,6 +39,7 @@ namespace cps {
 
 constexpr int kStages = 4;
 constexpr int kWaitLimit = 1 << 18;
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
 __host__ __device__ constexpr int a128(int b) { return (b + 127) / 128 * 128; }
 
@@ -49,11 +58,39 @@ struct TileXYZ {
     int bx, by, bz;  // tile index along x (32 columns), y (BY rows), z (kc planes)
 };
 
+__device__ __forceinline__ uint64_t globaltimer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ bool wait_stage(uint64_t *bar, uint32_t phase)
 {
-    for (int it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, phase)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    for (int it = 1; it < kWaitLimit; ++it) {
         if (mbar_try_wait(bar, phase)) return true;
+        if ((it & 255) == 0 && globaltimer_ns() - t0 > kWaitNs) return false;
+    }
     return false;
+}
+
+// After a wait gave up: thread 0 waits (bounded) for the planes [pl0, pl1]
+// of the tile whose loads may still be in flight (the plane that gave up has
+// had its whole limit already)
+__device__ __forceinline__ void drain_stages(uint64_t *full, uint32_t c0, int pl0, int pl1)
+{
+    for (int pl = pl0; pl <= pl1; ++pl) {
+        const uint32_t q = c0 + (uint32_t)pl;
+        wait_stage(&full[q % kStages], (q / kStages) & 1u);
+    }
+}
+
+// the test setting err[1] (extra bytes the first plane of a tile expects)
+__device__ __forceinline__ uint32_t wait_skew(const int *err)
+{
+    return (uint32_t)*(const volatile int *)(err + 1);
 }
 
 // 128-byte aligned start of the dynamic shared window (SMEM holds 128 spare bytes)
@@ -100,11 +137,13 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
     const bool rowok = j >= 1 && j < d.ny;
     const bool act = rowok && i >= 1 && i < d.nx;
     const uint32_t c0 = ctr;
+    const int npl = k1 - k0;
+    const uint32_t skew = tid == 0 ? wait_skew(err) : 0u;
     auto issue = [&](int pl, int k) {
         const int s = (int)((c0 + (uint32_t)pl) % kStages);
         unsigned char *b = sm + s * L::STAGE_B;
         fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
-        mbar_expect_tx(&full[s], L::TX);
+        mbar_expect_tx(&full[s], L::TX + (pl == 0 ? skew : 0u));
         for (int c = 0; c < 3; ++c) tma_load_3d(b + c * L::HALO_B, &M.halo[3 + c], &full[s], x0 - 4, y0 - 1, k);
         for (int c = 0; c < 3; ++c) tma_load_3d(b + 3 * L::HALO_B + c * L::OWN_B, &M.own[c], &full[s], x0, y0, k);
         tma_load_3d(b + 3 * L::HALO_B + 3 * L::OWN_B, &M.id, &full[s], x0, y0, k);
@@ -148,7 +187,10 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         const int s = (int)(q % kStages);
         const bool ok = wait_stage(&full[s], (q / kStages) & 1u);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(err, 1);
+            if (tid == 0) {
+                atomicExch(err, 1);
+                drain_stages(full, c0, it + 1, min(it + kStages - 1, npl - 1));
+            }
             return false;
         }
         const unsigned char *b = sm + s * L::STAGE_B;
@@ -212,11 +254,13 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
     const bool rowok = j < d.ny;
     const bool act = rowok && i < d.nx;
     const uint32_t c0 = ctr;
+    const int npl = k1 - k0;  // planes k0..k1 go through the ring (E one past the last H plane)
+    const uint32_t skew = tid == 0 ? wait_skew(err) : 0u;
     auto issue = [&](int pl, int k) {
         const int s = (int)((c0 + (uint32_t)pl) % kStages);
         unsigned char *b = sm + s * L::STAGE_B;
         fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
-        mbar_expect_tx(&full[s], L::TX);
+        mbar_expect_tx(&full[s], L::TX + (pl == 0 ? skew : 0u));
         for (int c = 0; c < 3; ++c) tma_load_3d(b + c * L::HALO_B, &M.halo[c], &full[s], x0, y0, k);
         for (int c = 0; c < 3; ++c) tma_load_3d(b + 3 * L::HALO_B + c * L::OWN_B, &M.own[3 + c], &full[s], x0, y0, k);
         tma_load_3d(b + 3 * L::HALO_B + 3 * L::OWN_B, &M.id, &full[s], x0, y0, k);
@@ -233,7 +277,10 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
     {
         const bool ok = wait_stage(&full[s0], (c0 / kStages) & 1u);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(err, 2);
+            if (tid == 0) {
+                atomicExch(err, 2);
+                drain_stages(full, c0, 1, min(kStages - 1, npl));
+            }
             return false;
         }
     }
@@ -249,7 +296,10 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
         const int s = (int)(q % kStages), sn = (int)(qn1 % kStages);
         const bool ok = wait_stage(&full[sn], (qn1 / kStages) & 1u);
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(err, 2);
+            if (tid == 0) {
+                atomicExch(err, 2);
+                drain_stages(full, c0, it + 2, min(it + kStages - 1, npl));
+            }
             return false;
         }
         const unsigned char *b = sm + s * L::STAGE_B, *bn = sm + sn * L::STAGE_B;

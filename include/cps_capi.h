@@ -341,8 +341,19 @@ CPS_API cps_status cps_grid_energy(cps_grid *g, double *electric, double *magnet
 /* an 8-bit RGB PNG of rgb[y][x][3] */
 CPS_API cps_status cps_png_rgb(const char *path, int32_t nx, int32_t ny, const uint8_t *rgb);
 /* reset fields, auxiliary state, port samples and DFT accumulators to zero
- * (initial populations for gain) and the step index to n0 */
+ * (initial populations for gain) and the step index to n0; also clears a
+ * device timeout (CPS_E_TIMEOUT) recorded by an earlier sweep */
 CPS_API cps_status cps_grid_reset(cps_grid *g, int64_t n0);
+/* test setting for the bounded device waits (no reference counterpart; the
+ * reference has no failure handling, main.cpp:68-85): with extra_bytes > 0
+ * (at most 4096) the first plane of every tile of this grid's own TMA sweeps
+ * (cps_step FUSED below the chunked size, cps_op_* and recorded steps)
+ * expects that many more bytes than its loads bring, so each block's wait
+ * runs out after its limit (about a second) and the step reports
+ * CPS_E_TIMEOUT at the next synchronisation, with no fault and the context
+ * intact.  0 (the default) restores normal operation; cps_grid_reset then
+ * makes the grid usable again. */
+CPS_API cps_status cps_grid_set_wait_skew(cps_grid *g, int32_t extra_bytes);
 /* count of non-finite field values (device reduction) */
 CPS_API cps_status cps_grid_check_finite(cps_grid *g, int64_t *nonfinite);
 /* FP64 gain populations, [ncells][4] N0..N3, cells in (i,j,k) order */
