@@ -46,7 +46,7 @@ class GridDesc(C.Structure):
 
 class PmlParams(C.Structure):
     _fields_ = [("npml", C.c_int32 * 6), ("m", C.c_double), ("malp", C.c_double), ("kapmax", C.c_double),
-                ("sig_ratio", C.c_double), ("alpmax", C.c_double)]
+                ("sig_ratio", C.c_double), ("alpmax", C.c_double), ("literal", C.c_int32)]
 
 
 class DlParams(C.Structure):
@@ -321,7 +321,8 @@ class Grid:
         return out
 
     def pml_init(self, p):
-        pp = PmlParams((C.c_int32 * 6)(*p["npml"]), p["m"], p["malp"], p["kapmax"], p["sig_ratio"], p["alpmax"])
+        pp = PmlParams((C.c_int32 * 6)(*p["npml"]), p["m"], p["malp"], p["kapmax"], p["sig_ratio"], p["alpmax"],
+                       int(p.get("literal", 0)))
         _check(self.L.cps_pml_init(self.h, C.byref(pp)))
 
     def dl_init(self, d):

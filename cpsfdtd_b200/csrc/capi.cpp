@@ -925,6 +925,7 @@ extern "C" cps_status cps_pml_init(cps_grid *g, const cps_pml_params *pp)
         REQUIRE(n1 >= 1 && 2 * n1 < nax[a] - 1, CPS_E_INVALID, "cps_pml_init: thickness must be >= 1 and leave an interior");
     }
     REQUIRE(pp->m >= 0 && pp->kapmax >= 1.0 && pp->alpmax >= 0, CPS_E_INVALID, "cps_pml_init: bad grading parameters");
+    REQUIRE(pp->literal == 0 || pp->literal == 1, CPS_E_INVALID, "cps_pml_init: literal must be 0 or 1");
     g->pml = *pp;
     const double eta0 = sqrt(kMu0 / kEps0);
     const double del[3] = {g->desc.dx, g->desc.dy, g->desc.dz};

@@ -11,6 +11,25 @@ namespace cps {
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 
+// Coefficient of a cell's psi term.  By default the cell's own curl
+// coefficient: bE of its medium, the Drude-Lorentz C3 on ID-2 cells (p.ce_disp),
+// bH of its medium on the H side -- the CFS-PML update for any medium, and
+// equal to the reference's values wherever the CPML holds eps_r = mu_r = 1
+// media.  With p.literal the reference's single coefficients dt/eps0 and
+// bH[0] (CPML.cpp:524-525), which make the CPML grow without bound when its
+// medium has eps_r != 1.
+template <typename T>
+__device__ __forceinline__ T pml_ce_cell(const PmlView<T> &p, const T *bE_table, int id)
+{
+    if (p.literal) return p.cpmlE;
+    return id == CPS_ID_DISPERSIVE ? p.ce_disp : __ldg(&bE_table[id]);
+}
+template <typename T>
+__device__ __forceinline__ T pml_ch_cell(const PmlView<T> &p, const T *bH_table, int id)
+{
+    return p.literal ? p.cpmlH : __ldg(&bH_table[id]);
+}
+
 // One component of the Drude-Lorentz ADE at one cell: Drude_Lorentz.cpp:163-184.
 // curl is the curl term already multiplied by C3; the state words of this
 // component are st[w * stride_cells], w = JD[nD] JL[nL] JL1[nL] E1.

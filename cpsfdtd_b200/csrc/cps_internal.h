@@ -103,7 +103,9 @@ struct PmlView {
     int np[6];
     const T *bE[6], *cE[6], *bH[6], *cH[6];
     T *qe[6][2], *qh[6][2];  // x slabs [k][j][s], y slabs [k][s][i], z slabs [s][j][i]
-    T cpmlE, cpmlH;
+    T cpmlE, cpmlH;  // the reference's single psi coefficients (literal mode)
+    T ce_disp;       // psi coefficient of ID-2 cells: the Drude-Lorentz C3 (bE[2] without Drude-Lorentz)
+    int literal;     // 1: cpmlE/cpmlH for every cell; 0: each cell's own curl coefficient
 };
 
 template <typename T>

@@ -270,6 +270,8 @@ inline PmlView<T> pml_view(const cps_grid *g)
     }
     p.cpmlE = (T)g->cpmlE;
     p.cpmlH = (T)g->cpmlH;
+    p.ce_disp = g->dl_on ? (T)g->dlc.C3 : (T)g->bE[CPS_ID_DISPERSIVE];
+    p.literal = g->pml.literal ? 1 : 0;
     return p;
 }
 

@@ -103,7 +103,7 @@ k_h_fused(FieldView<T> f, PmlView<T> p, int kc)
         T hy = aH * cur.hy - bH * dEx_k * ldg(&s.cHyx[k]) + bH * dEz_i * cHyz;
         T hz = aH * cur.hz + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
         if (PML && act) {
-            const T ch = p.cpmlH;
+            const T ch = pml_ch_cell(p, f.bH, (int)cur.id);
             if (fx >= 0) {
                 const int np = p.np[fx];
                 const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + sxl;
@@ -288,7 +288,7 @@ k_e_fused(FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc)
         }
         if (act) {
             if (PML) {
-                const T ce = p.cpmlE;
+                const T ce = pml_ce_cell(p, f.bE, id);
                 if (fx >= 0) {
                     const int np = p.np[fx];
                     const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + sxl;

@@ -79,7 +79,7 @@ __global__ void k_e_pml_face(FieldView<T> f, PmlView<T> p, int face)
     }
     const int cs = end == 0 ? s + 1 : s;  // coefficient index (CPML.cpp:534, 546)
     const int64_t g = d.idx(i, j, k), q = psi_index(d, axis, np, cs, i, j, k);
-    const T b = p.bE[face][cs], c = p.cE[face][cs], ce = p.cpmlE;
+    const T b = p.bE[face][cs], c = p.cE[face][cs], ce = pml_ce_cell(p, f.bE, (int)f.id[g]);
     T *q0 = p.qe[face][0], *q1 = p.qe[face][1];
     if (axis == 0) {
         q0[q] = b * q0[q] + c * (f.Hz[g] - f.Hz[g - 1]);
@@ -120,7 +120,7 @@ __global__ void k_h_pml_face(FieldView<T> f, PmlView<T> p, int face)
         k = end == 0 ? s : d.nz - np + s;
     }
     const int64_t g = d.idx(i, j, k), q = psi_index(d, axis, np, s, i, j, k);
-    const T b = p.bH[face][s], c = p.cH[face][s], ch = p.cpmlH;
+    const T b = p.bH[face][s], c = p.cH[face][s], ch = pml_ch_cell(p, f.bH, (int)f.id[g]);
     T *q0 = p.qh[face][0], *q1 = p.qh[face][1];
     if (axis == 0) {
         q0[q] = b * q0[q] + c * (f.Ez[g + 1] - f.Ez[g]);

@@ -113,7 +113,7 @@ __device__ __forceinline__ void h_cell(const FieldView<T> &f, const PmlView<T> &
     hy = aH * hyt[hr] - bH * dEx_k * sv.cHyx[k] + bH * dEz_i * hc.cHyz;
     hz = aH * hzt[hr] + bH * dEx_j * hc.cHzx - bH * dEy_i * hc.cHzy;
     if (PML)
-        pml_h_cell_pre<T, STORE>(pout, d, pc, i, j, k, r, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz, store);
+        pml_h_cell_pre<T, STORE>(pout, d, pc, pml_ch_cell(pout, f.bH, id), i, j, k, r, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz, store);
     if (TFSF) {
         hx = hx + hs.x;
         hy = hy + hs.y;
@@ -292,7 +292,7 @@ __device__ __forceinline__ void step_body(const StepMaps &M, const FieldView<T> 
                     gain_warp(G, d, j, k, bx, act, id, ex, ey, ez);
                 }
                 if (act && !(DL && id == CPS_ID_DISPERSIVE)) {
-                    if (PML) pml_e_cell_pre(pin, d, pce, i, j, k, qe, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
+                    if (PML) pml_e_cell_pre(pin, d, pce, pml_ce_cell(pin, fo.bE, id), i, j, k, qe, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
                     fn.Ex[g] = ex; fn.Ey[g] = ey; fn.Ez[g] = ez;
                 } else if (!act && inarr) {
                     fn.Ex[g] = ex; fn.Ey[g] = ey; fn.Ez[g] = ez;

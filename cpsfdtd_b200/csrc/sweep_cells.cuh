@@ -52,11 +52,10 @@ __device__ __forceinline__ ColPml<T> col_pml_h(const PmlView<T> &p, const Dims &
 
 // CPML H corrections at one cell (CPML.cpp:617-682), x then y then z slabs
 template <typename T>
-__device__ __forceinline__ void pml_h_cell(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, int i, int j,
-                                           int k, T dEz_i, T dEy_i, T dEx_j, T dEz_j, T dEy_k, T dEx_k, T &hx,
+__device__ __forceinline__ void pml_h_cell(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, T ch, int i,
+                                           int j, int k, T dEz_i, T dEy_i, T dEx_j, T dEz_j, T dEy_k, T dEx_k, T &hx,
                                            T &hy, T &hz)
 {
-    const T ch = p.cpmlH;
     if (c.fx >= 0) {
         const int np = p.np[c.fx];
         const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + c.sxl;
@@ -91,11 +90,10 @@ __device__ __forceinline__ void pml_h_cell(const PmlView<T> &p, const Dims &d, c
 
 // CPML E corrections at one cell (CPML.cpp:537-602), x then y then z slabs
 template <typename T>
-__device__ __forceinline__ void pml_e_cell(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, int i, int j,
-                                           int k, T dHz_i, T dHy_i, T dHx_j, T dHz_j, T dHy_k, T dHx_k, T &ex,
+__device__ __forceinline__ void pml_e_cell(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, T ce, int i,
+                                           int j, int k, T dHz_i, T dHy_i, T dHx_j, T dHz_j, T dHy_k, T dHx_k, T &ex,
                                            T &ey, T &ez)
 {
-    const T ce = p.cpmlE;
     if (c.fx >= 0) {
         const int np = p.np[c.fx];
         const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(np) + c.sxl;
@@ -180,11 +178,10 @@ __device__ __forceinline__ void psi_load_h(const PmlView<T> &p, const Dims &d, c
 
 // CPML E corrections with psi already in registers (same arithmetic as pml_e_cell)
 template <typename T>
-__device__ __forceinline__ void pml_e_cell_pre(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, int i, int j,
-                                               int k, const PsiRegs<T> &r, T dHz_i, T dHy_i, T dHx_j, T dHz_j,
+__device__ __forceinline__ void pml_e_cell_pre(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, T ce, int i,
+                                               int j, int k, const PsiRegs<T> &r, T dHz_i, T dHy_i, T dHx_j, T dHz_j,
                                                T dHy_k, T dHx_k, T &ex, T &ey, T &ez)
 {
-    const T ce = p.cpmlE;
     if (c.fx >= 0) {
         const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(p.np[c.fx]) + c.sxl;
         const T a0 = c.bx * r.x0 + c.cx * dHz_i, a1 = c.bx * r.x1 + c.cx * dHy_i;
@@ -215,11 +212,10 @@ __device__ __forceinline__ void pml_e_cell_pre(const PmlView<T> &p, const Dims &
 // CPML H corrections with psi already in registers (same arithmetic as
 // pml_h_cell); STORE = false computes the corrected H without writing psi
 template <typename T, bool STORE = true>
-__device__ __forceinline__ void pml_h_cell_pre(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, int i, int j,
-                                               int k, const PsiRegs<T> &r, T dEz_i, T dEy_i, T dEx_j, T dEz_j,
+__device__ __forceinline__ void pml_h_cell_pre(const PmlView<T> &p, const Dims &d, const ColPml<T> &c, T ch, int i,
+                                               int j, int k, const PsiRegs<T> &r, T dEz_i, T dEy_i, T dEx_j, T dEz_j,
                                                T dEy_k, T dEx_k, T &hx, T &hy, T &hz, bool store = true)
 {
-    const T ch = p.cpmlH;
     if (c.fx >= 0) {
         const int64_t q = ((int64_t)k * (d.ny + 1) + j) * psi_xw(p.np[c.fx]) + c.sxl;
         const T a0 = c.bx * r.x0 + c.cx * dEz_i, a1 = c.bx * r.x1 + c.cx * dEy_i;

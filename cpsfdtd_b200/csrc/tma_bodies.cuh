@@ -224,7 +224,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         // ID-2 cells are left untouched here: the Drude-Lorentz cell kernel
         // updates them (ADE, then CPML) after the sweep, in the reference order
         if (act && !(DL && id == CPS_ID_DISPERSIVE)) {
-            if (PML) pml_e_cell_pre(p, d, pc, i, j, k, qc, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
+            if (PML) pml_e_cell_pre(p, d, pc, pml_ce_cell(p, f.bE, id), i, j, k, qc, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
             const int64_t g = d.idx(i, j, k);
             f.Ex[g] = ex; f.Ey[g] = ey; f.Ez[g] = ez;
         }
@@ -318,7 +318,7 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
         T hy = aH * hyt[orow] - bH * dEx_k * sv.cHyx[k] + bH * dEz_i * cHyz;
         T hz = aH * hzt[orow] + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
         if (act) {
-            if (PML) pml_h_cell_pre(p, d, pc, i, j, k, qc, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz);
+            if (PML) pml_h_cell_pre(p, d, pc, pml_ch_cell(p, f.bH, id), i, j, k, qc, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz);
             const int64_t g = d.idx(i, j, k);
             f.Hx[g] = hx; f.Hy[g] = hy; f.Hz[g] = hz;
         }
@@ -389,7 +389,7 @@ __device__ __forceinline__ void dl_cell(const FieldView<T> &f, const FieldView<T
     }
     if (PML) {
         const ColPml<T> pc = col_pml_e(p, d, i, j, true);
-        pml_e_cell(p, d, pc, i, j, k, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
+        pml_e_cell(p, d, pc, pml_ce_cell(p, f.bE, CPS_ID_DISPERSIVE), i, j, k, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
     }
     f.Ex[g] = ex; f.Ey[g] = ey; f.Ez[g] = ez;
 }

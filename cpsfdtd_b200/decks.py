@@ -230,8 +230,10 @@ def dlambda_for_tau(lam: float, tau: float) -> float:
 
 
 def pml_params(n: int, m: float = 3.0, malp: float = 1.0, kapmax: float = 5.0,
-               sig_ratio: float = 1.0, alpmax: float = 0.05) -> dict:
-    return dict(npml=[n] * 6, m=m, malp=malp, kapmax=kapmax, sig_ratio=sig_ratio, alpmax=alpmax)
+               sig_ratio: float = 1.0, alpmax: float = 0.05, literal: int = 0) -> dict:
+    """CPML deck values; literal = 1 keeps the reference's single psi
+    coefficients (CPML.cpp:524-525), 0 each cell's own curl coefficient."""
+    return dict(npml=[n] * 6, m=m, malp=malp, kapmax=kapmax, sig_ratio=sig_ratio, alpmax=alpmax, literal=literal)
 
 
 def dl_params_metal() -> dict:

@@ -109,10 +109,17 @@ typedef struct cps_grid_desc {
 } cps_grid_desc;
 
 /* CPML deck values (CPML.cpp:37-62).  npml order x1 x2 y1 y2 z1 z2; both ends
- * of an axis must be equal and >= 1, or both 0 to leave that axis open. */
+ * of an axis must be equal and >= 1, or both 0 to leave that axis open.
+ * literal = 0 (default): each cell's psi term takes the cell's own curl
+ * coefficient (bE of its medium, the Drude-Lorentz C3 on ID-2 cells, bH of
+ * its medium on the H side), the CFS-PML update for any medium; it equals the
+ * reference wherever the CPML holds eps_r = mu_r = 1 media.  literal = 1 uses
+ * the reference's single dt/eps0 and bH[0] (CPML.cpp:524-525), with which the
+ * CPML grows without bound when its medium has eps_r != 1. */
 typedef struct cps_pml_params {
     int32_t npml[6];
     double m, malp, kapmax, sig_ratio, alpmax;
+    int32_t literal;
 } cps_pml_params;
 
 /* Drude-Lorentz deck values (Drude_Lorentz.cpp:37-94); frequencies in Hz.

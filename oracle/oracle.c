@@ -33,6 +33,7 @@ typedef struct {
     double *qe[6][2]; /* psi of H differences, applied to E (reference QH**) */
     double *qh[6][2]; /* psi of E differences, applied to H (reference QE**) */
     double cpmlE, cpmlH;
+    int literal; /* 1: cpmlE/cpmlH for every cell (CPML.cpp:524-525); 0: each cell's curl coefficient */
 } pml_t;
 
 typedef struct {
@@ -260,9 +261,10 @@ static void pml_grade_h(double *kappa, double *b, double *c, int first, int np, 
  * ends of an axis must be equal (the reference folds the second-end kappa
  * with the first-end count, CPML.cpp:374,402,430,459,487,515). */
 int orc_pml_init(orc *o, const int32_t npml[6], double m, double malp, double kapmax,
-                 double sig_ratio, double alpmax)
+                 double sig_ratio, double alpmax, int literal)
 {
     pml_t *P = &o->pml;
+    P->literal = literal;
     for (int a = 0; a < 3; ++a) {
         if (npml[2 * a] != npml[2 * a + 1]) return 1;
         if (npml[2 * a] < 1) return 1;
@@ -340,6 +342,22 @@ static inline int64_t qidx(const orc *o, int f, int s, int i, int j, int k)
     return ((int64_t)i * (o->ny + 1) + j) * (np + 1) + s;
 }
 
+/* Coefficient of a cell's psi term: with literal the reference's single
+ * cpmlE = dt/eps0 and cpmlH = bH[0] (CPML.cpp:524-525); otherwise the cell's
+ * own curl coefficient -- bE of its medium (C3 on Drude-Lorentz cells), bH
+ * of its medium -- which equals the literal values in eps_r = mu_r = 1 media. */
+static inline double pml_ce(const orc *o, int64_t g)
+{
+    if (o->pml.literal) return o->pml.cpmlE;
+    const int id = o->id[g];
+    return (id == ID_DISPERSIVE && o->dl.on) ? o->dl.C3 : o->bE[id];
+}
+
+static inline double pml_ch(const orc *o, int64_t g)
+{
+    return o->pml.literal ? o->pml.cpmlH : o->bH[o->id[g]];
+}
+
 /* CPML::UpdateCPMLEFields, CPML.cpp:529-607 */
 void orc_op_e_pml(orc *o)
 {
@@ -347,7 +365,6 @@ void orc_op_e_pml(orc *o)
     if (!P->on) return;
     double *Ex = o->F[EX], *Ey = o->F[EY], *Ez = o->F[EZ];
     const double *Hx = o->F[HX], *Hy = o->F[HY], *Hz = o->F[HZ];
-    const double ce = P->cpmlE;
     const int nx = o->nx, ny = o->ny, nz = o->nz;
     for (int end = 0; end < 2; ++end) { /* x slabs */
         const int f = FX1 + end, np = P->np[f];
@@ -361,9 +378,9 @@ void orc_op_e_pml(orc *o)
                 for (int k = 1; k < nz; ++k) {
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, cs, i, j, k);
                     q0[q] = b[cs] * q0[q] + c[cs] * (Hz[g] - Hz[g - o->sx]);
-                    Ey[g] = Ey[g] - q0[q] * ce;
+                    Ey[g] = Ey[g] - q0[q] * pml_ce(o, g);
                     q1[q] = b[cs] * q1[q] + c[cs] * (Hy[g] - Hy[g - o->sx]);
-                    Ez[g] = Ez[g] + q1[q] * ce;
+                    Ez[g] = Ez[g] + q1[q] * pml_ce(o, g);
                 }
         }
     }
@@ -379,9 +396,9 @@ void orc_op_e_pml(orc *o)
                 for (int k = 1; k < nz; ++k) {
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, cs, i, j, k);
                     q0[q] = b[cs] * q0[q] + c[cs] * (Hx[g] - Hx[g - o->sy]);
-                    Ez[g] = Ez[g] - q0[q] * ce;
+                    Ez[g] = Ez[g] - q0[q] * pml_ce(o, g);
                     q1[q] = b[cs] * q1[q] + c[cs] * (Hz[g] - Hz[g - o->sy]);
-                    Ex[g] = Ex[g] + q1[q] * ce;
+                    Ex[g] = Ex[g] + q1[q] * pml_ce(o, g);
                 }
             }
     }
@@ -397,9 +414,9 @@ void orc_op_e_pml(orc *o)
                     const int k = end == 0 ? s + 1 : nz - np + s;
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, cs, i, j, k);
                     q0[q] = b[cs] * q0[q] + c[cs] * (Hy[g] - Hy[g - 1]);
-                    Ex[g] = Ex[g] - q0[q] * ce;
+                    Ex[g] = Ex[g] - q0[q] * pml_ce(o, g);
                     q1[q] = b[cs] * q1[q] + c[cs] * (Hx[g] - Hx[g - 1]);
-                    Ey[g] = Ey[g] + q1[q] * ce;
+                    Ey[g] = Ey[g] + q1[q] * pml_ce(o, g);
                 }
     }
 }
@@ -411,7 +428,6 @@ void orc_op_h_pml(orc *o)
     if (!P->on) return;
     const double *Ex = o->F[EX], *Ey = o->F[EY], *Ez = o->F[EZ];
     double *Hx = o->F[HX], *Hy = o->F[HY], *Hz = o->F[HZ];
-    const double ch = P->cpmlH;
     const int nx = o->nx, ny = o->ny, nz = o->nz;
     for (int end = 0; end < 2; ++end) {
         const int f = FX1 + end, np = P->np[f];
@@ -424,9 +440,9 @@ void orc_op_h_pml(orc *o)
                 for (int k = 0; k < nz; ++k) {
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, s, i, j, k);
                     q0[q] = b[s] * q0[q] + c[s] * (Ez[g + o->sx] - Ez[g]);
-                    Hy[g] = Hy[g] + q0[q] * ch;
+                    Hy[g] = Hy[g] + q0[q] * pml_ch(o, g);
                     q1[q] = b[s] * q1[q] + c[s] * (Ey[g + o->sx] - Ey[g]);
-                    Hz[g] = Hz[g] - q1[q] * ch;
+                    Hz[g] = Hz[g] - q1[q] * pml_ch(o, g);
                 }
         }
     }
@@ -441,9 +457,9 @@ void orc_op_h_pml(orc *o)
                 for (int k = 0; k < nz; ++k) {
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, s, i, j, k);
                     q0[q] = b[s] * q0[q] + c[s] * (Ex[g + o->sy] - Ex[g]);
-                    Hz[g] = Hz[g] - q0[q] * ch;
+                    Hz[g] = Hz[g] - q0[q] * pml_ch(o, g);
                     q1[q] = b[s] * q1[q] + c[s] * (Ez[g + o->sy] - Ez[g]);
-                    Hx[g] = Hx[g] + q1[q] * ch;
+                    Hx[g] = Hx[g] + q1[q] * pml_ch(o, g);
                 }
             }
     }
@@ -458,9 +474,9 @@ void orc_op_h_pml(orc *o)
                     const int k = end == 0 ? s : nz - np + s;
                     const int64_t g = IDX(o, i, j, k), q = qidx(o, f, s, i, j, k);
                     q0[q] = b[s] * q0[q] + c[s] * (Ey[g + 1] - Ey[g]);
-                    Hx[g] = Hx[g] - q0[q] * ch;
+                    Hx[g] = Hx[g] - q0[q] * pml_ch(o, g);
                     q1[q] = b[s] * q1[q] + c[s] * (Ex[g + 1] - Ex[g]);
-                    Hy[g] = Hy[g] + q1[q] * ch;
+                    Hy[g] = Hy[g] + q1[q] * pml_ch(o, g);
                 }
     }
 }

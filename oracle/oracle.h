@@ -57,8 +57,11 @@ int orc_set_threads(int n);
 int orc_set_media(orc *o, int n, const double *epsR, const double *muR,
                   const double *sig, const double *sigM);
 int orc_set_ids(orc *o, const uint8_t *ids);
+/* literal = 1: the reference's single psi coefficients dt/eps0 and bH[0]
+ * (CPML.cpp:524-525); 0: each cell's own curl coefficient (equal to them in
+ * eps_r = mu_r = 1 media, the CFS-PML form in any medium) */
 int orc_pml_init(orc *o, const int32_t npml[6], double m, double malp,
-                 double kapmax, double sig_ratio, double alpmax);
+                 double kapmax, double sig_ratio, double alpmax, int literal);
 /* literal = 1 takes C1 and C5 exactly as Drude_Lorentz.cpp:96,106; 0 (the
  * default of the product) takes the values the ADE discretisation gives;
  * 2 (one Drude pole, no Lorentz pole) is the single-pole Drude class with the

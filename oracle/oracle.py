@@ -47,7 +47,8 @@ def lib():
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_media.argtypes = [P, C.c_int, dp, dp, dp, dp]
         L.orc_set_ids.argtypes = [P, C.c_void_p]
-        L.orc_pml_init.argtypes = [P, C.POINTER(C.c_int32), C.c_double, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_pml_init.argtypes = [P, C.POINTER(C.c_int32), C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_int]
         L.orc_dl_init.argtypes = [P, C.c_double, C.c_double, C.c_int, dp, dp, C.c_int, dp, dp, dp, C.c_int]
         L.orc_gain_init.argtypes = [P, C.c_int] + [C.c_double] * 10
         L.orc_tfsf_init.argtypes = [P, C.POINTER(TfsfParams)]
@@ -119,7 +120,8 @@ class Oracle:
         if dk.pml:
             p = dk.pml
             n = (C.c_int32 * 6)(*p["npml"])
-            assert o.L.orc_pml_init(o.h, n, p["m"], p["malp"], p["kapmax"], p["sig_ratio"], p["alpmax"]) == 0
+            assert o.L.orc_pml_init(o.h, n, p["m"], p["malp"], p["kapmax"], p["sig_ratio"], p["alpmax"],
+                                    int(p.get("literal", 0))) == 0
         if dk.dl:
             d = dk.dl
             a = [_dp(d[k]) for k in ("fD", "gD", "fL", "dL", "depsL")]

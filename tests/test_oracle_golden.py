@@ -28,7 +28,7 @@ def _ids_and_ports(dk):
 @pytest.mark.parametrize("name", sorted(gc.CASES_3D))
 def test_oracle_matches_reference_3d(name, oracle_mod):
     g = GOLDEN["cases3d"][name]
-    dk = gc.CASES_3D[name]()
+    dk = gc.literal_pml(gc.CASES_3D[name]())
     ids, pts = _ids_and_ports(dk)
     assert sha(ids) == g["ids"]["sha256"], "rasteriser differs from Structure::generate_mesh"
     for p, gp in zip(pts, g["ports"]):

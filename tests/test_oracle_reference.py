@@ -10,7 +10,7 @@ import golden.golden_cases as gc
 
 
 def test_port_dft_matches_dft_of_reference_series(oracle_mod, have_ref):
-    dk = gc.c2_small()
+    dk = gc.literal_pml(gc.c2_small())
     ref = oracle_mod.run_ref_harness(dk, record_ports=True)
     pts = [p["points"] for p in ref["ports"]]
     o = oracle_mod.Oracle.from_deck(dk, ref["ids"], pts)
@@ -30,7 +30,7 @@ def test_port_dft_matches_dft_of_reference_series(oracle_mod, have_ref):
 
 
 def test_oracle_matches_reference_midsize(oracle_mod, have_ref):
-    dk = decks.config2(n=56, steps=40, nfreq=2)
+    dk = gc.literal_pml(decks.config2(n=56, steps=40, nfreq=2))
     ref = oracle_mod.run_ref_harness(dk)
     o = oracle_mod.Oracle.from_deck(dk, ref["ids"], [p["points"] for p in ref["ports"]])
     o.step(dk.nsteps)
