@@ -1,23 +1,38 @@
 #!/usr/bin/env python
 """bench.py -- throughput of the cpsFDTD time-stepping loop on B200.
 
-Workload (default): the dispersive-scattering deck -- 256^3 cells, dx 5 nm,
-CPML 12, TF/SF Gaussian beam (inset 20, 550 nm, theta 30, phi 45, pulse
-tau 4 fs), 4x4x4 Drude-Lorentz spheres (r 15, pitch 40), six planar ports with
-64-frequency FP64 DFTs; FP32 fields, fused path.  One bench step = one whole
-job of --job-steps time steps (default 4000) from a reset state, ports flushed.
-Synthetic geometry from the seeded deck generator; no dataset.
+Headline workload (default, the largest single-GPU configuration): the
+disordered photonic-crystal laser -- 384^3 cells, dx 10 nm, CPML 16, eps 11.9
+spheres (r 8, pitch 30, jittered +-4) in an eps 2.25 background doped with
+four-level gain, Ez seed pulse, spherical port r 150 with a 32-frequency FP64
+DFT; 20000-step jobs.  FP32 fields, FP64 port accumulators, fused path.  One
+bench step = --chunk time steps of the job (default 500; the job restarts
+from its initial state after its last step).  Synthetic geometry from the
+seeded deck generator; no dataset.
 
-Metric: Gcell-upd/s = cells x time steps / time, whole job, all ranks.
-  value  : device-timed (CUDA events on the grid's stream), inputs in HBM
-  e2e    : through the C ABI from host buffers: grid setup from the deck and
-           the host ID grid, the run, and the port spectra read back to host
-  roofline: the E sweep (dominant kernel) algorithmic bytes / its mean
-           event-timed duration (events around each sweep of one job run
-           after the timed region), against the measured HBM copy bandwidth
-  cpu_baseline: the reference's own OpenMP code (oracle/_ref/ref_bench; its
-           3-D Drude-Lorentz from the oracle restatement) on the same deck
-Multi-GPU: one replica job per rank (the path does not shard), weak scaling.
+Metric: Gcell-upd/s = cells x time steps / time, all ranks.
+  value    : device-timed (CUDA events on the grid's stream), inputs in HBM
+  e2e      : through the C ABI from host buffers: per e2e step one whole job
+             (grid set-up from the host deck, IDs and port points in pinned
+             memory, all its time steps, port spectra read back to pinned
+             memory)
+  fp64     : the same deck in FP64 on the plain path (one kernel per
+             reference routine) and on the fused path, value and e2e
+  roofline : the E sweep (dominant kernel), algorithmic bytes / its mean
+             event-timed duration, against the measured HBM copy bandwidth;
+             bytes counted as each field word of the swept side read and
+             written once + 1 B ID + CPML psi + gain/Drude-Lorentz state,
+             and (printed beside) the two-sweep count that adds the other
+             side's field read
+  c2       : the dispersive-scattering deck (256^3, Drude-Lorentz spheres,
+             TF/SF beam, six 64-frequency ports, 4000-step jobs) beside it
+  accuracy : each chosen form against FP64 per config -- field relative L2,
+             port-spectrum relative error, resonance-frequency shift
+  cpu_baseline: the reference's own OpenMP code (oracle/_ref/ref_bench; the
+             3-D gain and Drude-Lorentz from the oracle restatement)
+  ensemble : 256 uneven grids (C4) batched vs one grid per launch
+  serving  : a Poisson job stream (C5) served vs one job at a time
+Multi-GPU: one replica per rank (the path does not shard), weak scaling.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -29,7 +44,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -54,27 +68,45 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=256, help="grid edge (cells)")
-    ap.add_argument("--workload", default="dispersive", choices=["dispersive", "laser"],
-                    help="bench deck: dispersive scattering (default) or the photonic-crystal laser")
-    ap.add_argument("--job-steps", type=int, default=4000)
+    ap.add_argument("--workload", default="laser", choices=["laser", "dispersive"],
+                    help="headline deck: the photonic-crystal laser (default) or the dispersive scattering deck")
+    ap.add_argument("--n", type=int, default=0, help="grid edge (cells); 0: the workload's own (384 / 256)")
+    ap.add_argument("--job-steps", type=int, default=0, help="time steps per job; 0: the workload's own")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="time steps per bench step; 0: 500 for the laser deck, a whole job for the dispersive one")
     ap.add_argument("--path", default="fused", choices=["fused", "onepass"],
                     help="one-grid stepping path: two TMA sweeps per step (default) or the one-pass step")
-    ap.add_argument("--e2e-steps", type=int, default=2, help="end-to-end jobs to time")
+    ap.add_argument("--e2e-jobs", type=int, default=1, help="whole jobs of the end-to-end leg")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 legs")
+    ap.add_argument("--fp64-chunks", type=int, default=2, help="timed bench steps of each FP64 leg")
+    ap.add_argument("--fp64-e2e-steps", type=int, default=1000,
+                    help="time steps of the FP64 end-to-end job (set-up + steps + read-back)")
+    ap.add_argument("--no-c2", action="store_true", help="skip the dispersive-scattering deck beside the headline")
+    ap.add_argument("--c2-jobs", type=int, default=3, help="timed 4000-step jobs of the C2 leg")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the accuracy legs")
+    ap.add_argument("--acc-c3-steps", type=int, default=2000, help="time steps of the C3 accuracy sample")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-steps", type=int, default=3, help="time steps in the CPU baseline sample")
     ap.add_argument("--ens-grids", type=int, default=256, help="grids of the batched ensemble leg (0: skip)")
     ap.add_argument("--ens-steps", type=int, default=128, help="timed steps of the batched ensemble")
-    ap.add_argument("--ens-loop-steps", type=int, default=8,
+    ap.add_argument("--ens-loop-steps", type=int, default=64,
                     help="steps per grid of the one-grid-per-launch comparison loops")
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving leg (0: skip)")
-    ap.add_argument("--serve-step-scale", type=float, default=2.0,
+    ap.add_argument("--serve-step-scale", type=float, default=1.0,
                     help="job step counts are the log-uniform [500, 20000] draws divided by this")
     ap.add_argument("--serve-tile", default="",
                     help="batch tile of the serving loop as rows,planes,mode (empty: the library default)")
     ap.add_argument("--serve-load", type=float, default=2.0,
                     help="offered load: arrival rate x job work / 20 Gcell-upd/s")
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.n == 0:
+        a.n = 384 if a.workload == "laser" else 256
+    if a.job_steps == 0:
+        a.job_steps = 20000 if a.workload == "laser" else 4000
+    if a.chunk == 0:
+        a.chunk = 500 if a.workload == "laser" else a.job_steps
+    a.chunk = min(a.chunk, a.job_steps)
+    return a
 
 
 class Clocks:
@@ -125,30 +157,61 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def workload(n, job_steps, kind="dispersive"):
-    """The bench deck: the dispersive-scattering deck (default), or the
-    disordered photonic-crystal laser deck (four-level gain, 32-frequency
-    spherical-port DFT)."""
+# ------------------------------------------------------------------ decks
+
+def workload(kind, n, job_steps):
+    """The bench decks: the disordered photonic-crystal laser (four-level
+    gain, 32-frequency spherical-port DFT) or the dispersive-scattering deck
+    (Drude-Lorentz spheres, TF/SF beam, six 64-frequency planar ports)."""
     from cpsfdtd_b200 import decks
     if kind == "laser":
         return decks.config3(n=n, steps=job_steps, seed=0, nfreq=32)
     return decks.config2(n=n, steps=job_steps, nfreq=64)
 
 
-def workload_name(dk, kind):
+def workload_name(dk, kind, chunk):
+    step = (f"1 bench step = {chunk} time steps of a {dk.nsteps}-step job" if chunk < dk.nsteps
+            else f"1 bench step = 1 job of {dk.nsteps} time steps")
     if kind == "laser":
         return (f"disordered photonic-crystal laser {dk.nx}^3, eps 11.9 spheres in gain-doped eps 2.25, CPML "
-                f"{dk.pml['npml'][0]}, Ez seed pulse, spherical port x 32-freq FP64 DFT; 1 bench step = 1 job of "
-                f"{dk.nsteps} time steps")
+                f"{dk.pml['npml'][0]}, Ez seed pulse, spherical port x 32-freq FP64 DFT; {step}")
     return (f"dispersive scattering {dk.nx}^3, Drude-Lorentz 4x4x4 spheres, CPML {dk.pml['npml'][0]}, TF/SF "
-            f"Gaussian beam, 6 ports x 64-freq FP64 DFT; 1 bench step = 1 job of {dk.nsteps} time steps")
+            f"Gaussian beam, 6 ports x 64-freq FP64 DFT; {step}")
 
 
-def config_of(dk, kind, world, path="fused"):
-    return {"workload": workload_name(dk, kind), "grid": [dk.nx, dk.ny, dk.nz], "time_steps_per_job": dk.nsteps,
-            "precision": "fp32 fields, fp64 port accumulators", "path": path,
+def config_of(dk, kind, world, chunk, path="fused"):
+    return {"workload": workload_name(dk, kind, chunk), "grid": [dk.nx, dk.ny, dk.nz],
+            "time_steps_per_job": dk.nsteps, "time_steps_per_bench_step": chunk,
+            "precision": "fp32 fields, fp32 gain state (population offsets), fp64 port accumulators"
+            if kind == "laser" else "fp32 fields, fp64 port accumulators", "path": path,
             "l2": f"inputs larger than L2 (fields {6 * 4 * (dk.nx + 1) * (dk.ny + 1) * (dk.nz + 1) / 1e9:.2f} GB "
                   "per grid)", "parallelism": f"replicas x{world}"}
+
+
+class Prepared:
+    """A deck with its host inputs (IDs, port points) and aux cell counts."""
+
+    def __init__(self, kind, n, job_steps):
+        import cpsfdtd_b200 as cps
+        from cpsfdtd_b200 import decks
+        self.kind = kind
+        self.dk = workload(kind, n, job_steps)
+        dk = self.dk
+        self.ids = dk.ids if dk.ids is not None else cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz,
+                                                                   dk.shapes)
+        self.pts = [cps.port_points(dk, p) for p in dk.ports]
+        inner = self.ids[1:-1, 1:-1, 1:-1]
+        self.ndl = int((inner == decks.ID_DISPERSIVE).sum()) if dk.dl else 0
+        self.ngain = int((inner == decks.ID_GAIN).sum()) if dk.gain else 0
+
+    def grid(self, prec, device, ids=None):
+        import cpsfdtd_b200 as cps
+        return cps.Grid.from_deck(self.dk, prec, ids=self.ids if ids is None else ids, port_points_list=self.pts,
+                                  device=device)
+
+    @property
+    def cells(self):
+        return self.dk.nx * self.dk.ny * self.dk.nz
 
 
 def aggregate(units_local, ms_local, dist=None, device=None):
@@ -166,11 +229,17 @@ def aggregate(units_local, ms_local, dist=None, device=None):
 
 
 def sweep_bytes(dk, ndl, prec_bytes=4, ngain=0):
-    """Algorithmic bytes of one H sweep and one E sweep (FP32): each field word
-    read and written once, 1 B material ID, CPML psi (2 words read+write per
-    slab cell per sweep), Drude-Lorentz state (3 x (nD + 2 nL + 1) words read
-    + write per ID-2 cell), gain state (12 polarisation + 3 population words
-    read + write per gain cell).  Neighbour re-reads are not counted."""
+    """Algorithmic bytes of one H sweep and one E sweep.  Returns two models as
+    ((h, e), (h2, e2)):
+      model 1: each field word of the swept side read and written once
+               (3 x 2 x s), 1 B material ID, CPML psi (2 words read + write
+               per slab cell of that side), Drude-Lorentz state (3 x (nD +
+               2 nL + 1) words read + write per ID-2 cell, E side), gain state
+               (12 polarisation + 3 population words read + write per gain
+               cell, E side) -- a step is 50 B per cell at s = 4 plus aux;
+      model 2: model 1 plus the read of the other side's three components,
+               which a design with separate H and E sweeps makes every sweep.
+    Neighbour and halo re-reads are not counted in either."""
     nx, ny, nz, s = dk.nx, dk.ny, dk.nz, prec_bytes
     np_ = dk.pml["npml"][0] if dk.pml else 0
     h_cells = nx * ny * nz
@@ -178,19 +247,19 @@ def sweep_bytes(dk, ndl, prec_bytes=4, ngain=0):
     h_slab = 2 * np_ * (ny * nz + nx * nz + nx * ny)
     e_slab = 2 * np_ * ((ny - 1) * (nz - 1) + (nx - 1) * (nz - 1) + (nx - 1) * (ny - 1))
     psi = 2 * 2 * s
-    h = h_cells * (9 * s + 1) + h_slab * psi
+    h = h_cells * (6 * s + 1) + h_slab * psi
     stride = len(dk.dl["fD"]) + 2 * len(dk.dl["fL"]) + 1 if dk.dl else 0
-    e = e_cells * (9 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s + ngain * 15 * 2 * s
-    return h, e
+    e = e_cells * (6 * s + 1) + e_slab * psi + ndl * 3 * stride * 2 * s + ngain * 15 * 2 * s
+    return (h, e), (h + h_cells * 3 * s, e + e_cells * 3 * s)
 
 
 def onepass_bytes(dk, ngain, prec_bytes=4):
-    """Algorithmic bytes of one one-pass sweep (FP32): the six fields read and
-    written once, 1 B ID, CPML psi of both sides (2 words read + write per slab
-    cell and side), gain state; the Drude-Lorentz cells run in their own kernel."""
-    h, e = sweep_bytes(dk, 0, prec_bytes, ngain)
+    """Algorithmic bytes of one one-pass sweep: the six fields read and written
+    once, 1 B ID, CPML psi of both sides, gain state (Drude-Lorentz cells run
+    in their own kernel)."""
+    (h, e), _ = sweep_bytes(dk, 0, prec_bytes, ngain)
     nx, ny, nz, s = dk.nx, dk.ny, dk.nz, prec_bytes
-    return h + e - nx * ny * nz * (9 * s + 1) - (nx - 1) * (ny - 1) * (nz - 1) * (9 * s + 1) + nx * ny * nz * (12 * s + 1)
+    return h + e - nx * ny * nz * (6 * s + 1) - (nx - 1) * (ny - 1) * (nz - 1) * (6 * s + 1) + nx * ny * nz * (12 * s + 1)
 
 
 def dist_setup():
@@ -207,61 +276,48 @@ def dist_setup():
     return world, rank, local, dist
 
 
-def cpu_baseline(dk, steps, deck_kind="dispersive"):
-    """The reference's own code on the same deck, bounded sample on all host cores."""
+# ------------------------------------------------------------ CPU legs
+
+def cpu_run(dk, ids, warm, steps, kind):
+    """The reference's own code on the deck (oracle/_ref/ref_bench) on all host
+    cores, or the oracle restatement when the reference build is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     threads = os.cpu_count() or 1
+    extra = "3-D four-level gain" if kind == "laser" else "3-D Drude-Lorentz"
     if os.path.exists(oracle.REF_BENCH):
-        r = oracle.ref_bench(dk, 1, steps, threads=threads)
-        kind = "reference"
-        extra = "3-D Drude-Lorentz" if deck_kind == "dispersive" else "3-D four-level gain"
-        sample = (f"{dk.nx}^3 deck, {steps} time steps after 1 warm-up, reference BasicFDTD/CPML/TF_SF/Ports "
-                  f"(OpenMP) + {extra} from the oracle restatement")
-    else:
-        o = oracle.Oracle.from_deck(dk, _ids(dk))
-        oracle.Oracle.threads(threads)
-        o.step(1)
-        t0 = time.perf_counter()
-        o.step(steps)
-        r = {"cells": dk.cells, "steps": steps, "seconds": time.perf_counter() - t0, "threads": threads}
-        kind = "port"
-        sample = f"{dk.nx}^3 deck, {steps} time steps after 1 warm-up, oracle restatement (OpenMP)"
-    gcell = r["cells"] * r["steps"] / r["seconds"] / 1e9
-    return {"value": gcell, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample}
+        r = oracle.ref_bench(dk, warm, steps, threads=threads)
+        what = f"reference BasicFDTD/CPML/TF_SF/Ports (OpenMP) + {extra} from the oracle restatement"
+        return r, "reference", what
+    o = oracle.Oracle.from_deck(dk, ids)
+    oracle.Oracle.threads(threads)
+    o.step(warm)
+    t0 = time.perf_counter()
+    o.step(steps)
+    r = {"cells": dk.cells, "steps": steps, "seconds": time.perf_counter() - t0, "threads": threads}
+    return r, "port", "oracle restatement (OpenMP)"
 
 
-_IDS = {}
-
-
-def _ids(dk):
-    import cpsfdtd_b200 as cps
-    key = (dk.nx, dk.ny, dk.nz)
-    if key not in _IDS:
-        _IDS[key] = dk.ids if dk.ids is not None else cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
-    return _IDS[key]
+def cpu_baseline(prep, steps):
+    try:
+        r, kind, what = cpu_run(prep.dk, prep.ids, 1, steps, prep.kind)
+    except Exception as ex:  # the baseline is reported, never required
+        return {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": f"failed: {ex}"}
+    return {"value": r["cells"] * r["steps"] / r["seconds"] / 1e9, "unit": "Gcell-upd/s", "cores": r["threads"],
+            "kind": kind, "sample": f"{prep.dk.nx}^3 {prep.kind} deck, {steps} time steps after 1 warm-up, {what}"}
 
 
 def run_reference(args):
     world, rank, local, dist = dist_setup()
     if rank != 0:
         return
-    dk = workload(args.n, args.job_steps, args.workload)
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    threads = os.cpu_count() or 1
-    if os.path.exists(oracle.REF_BENCH):
-        r = oracle.ref_bench(dk, args.warmup, args.steps, threads=threads)
-        extra = "3-D Drude-Lorentz" if args.workload == "dispersive" else "3-D four-level gain"
-        kind, what = "reference", f"reference BasicFDTD/CPML/TF_SF/Ports (OpenMP) + {extra} from the oracle restatement"
-    else:
-        o = oracle.Oracle.from_deck(dk, _ids(dk))
-        oracle.Oracle.threads(threads)
-        o.step(args.warmup)
-        t0 = time.perf_counter()
-        o.step(args.steps)
-        r = {"cells": dk.cells, "steps": args.steps, "seconds": time.perf_counter() - t0, "threads": threads}
-        kind, what = "port", "oracle restatement (OpenMP)"
+    dk = workload(args.workload, args.n, args.job_steps)
+    ids = dk.ids
+    if ids is None:
+        import cpsfdtd_b200 as cps
+        ids = cps.rasterize(dk.nx, dk.ny, dk.nz, dk.dx, dk.dy, dk.dz, dk.shapes)
+    r, kind, what = cpu_run(dk, ids, args.warmup, args.steps, args.workload)
     v = r["cells"] * r["steps"] / r["seconds"] / 1e9
     sample = (f"{dk.nx}^3 {args.workload} deck: each bench step is 1 time step of the job (bounded sample), "
               f"{args.steps} timed after {args.warmup} warm-up, {what}")
@@ -269,10 +325,240 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["seconds"] / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded deck generator)",
-            "config": config_of(dk, args.workload, args.gpus, args.path),
+            "config": config_of(dk, args.workload, args.gpus, args.chunk, args.path),
             "cpu_baseline": {"value": v, "unit": "Gcell-upd/s", "cores": r["threads"], "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "Gcell-upd/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ GPU legs
+
+class Stepper:
+    """Bench steps of `chunk` time steps over consecutive jobs of one grid: a
+    job that has run all its steps has its spectra flushed and restarts from
+    the initial state."""
+
+    def __init__(self, g, dk, chunk, path):
+        self.g, self.dk, self.chunk, self.path = g, dk, chunk, path
+        self.left = dk.nsteps
+
+    def step(self):
+        if self.left == 0:
+            self.g.flush_ports()
+            self.g.reset(self.dk.n0)
+            self.left = self.dk.nsteps
+        n = min(self.chunk, self.left)
+        self.g.step(n, self.path)
+        self.left -= n
+        return n
+
+
+def timed_chunks(g, st, warm, steps, dist=None, clocks=None):
+    """warm untimed bench steps, then `steps` timed with CUDA events on the
+    grid's stream (barrier + synchronize on both sides); returns (ms, time
+    steps, launches, clocks)."""
+    import torch
+    stream = torch.cuda.ExternalStream(g.stream(), device=torch.cuda.current_device())
+    for _ in range(warm):
+        st.step()
+    g.sync()
+    l0 = g.launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    nts = 0
+    for _ in range(steps):
+        nts += st.step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop() if clocks else None
+    return e0.elapsed_time(e1), nts, g.launches() - l0, clk
+
+
+def sweep_roofline(prep, g, path, value_per_gpu):
+    """Mean event-timed H and E sweep durations over 200 more time steps from
+    the reset state, run as the direct launch sequence (the timed steps replay
+    the same kernels in CUDA-graph chunks, where single launches are not
+    timed)."""
+    import cpsfdtd_b200 as cps
+    dk = prep.dk
+    g.reset(dk.n0)
+    g.set_timing(1)
+    g.step(min(200, dk.nsteps), path)
+    g.sync()
+    h_ms, e_ms, nsamp = g.timing()
+    g.set_timing(0)
+    P, src = peaks()
+    (hb, eb), (hb2, eb2) = sweep_bytes(dk, prep.ndl, ngain=prep.ngain)
+    if path == cps.ONEPASS:  # h_ms: the one-pass sweep (with its TF/SF terms); e_ms: the Drude-Lorentz cells
+        dom_ms, dom_b, dom_b2, dom = h_ms, onepass_bytes(dk, prep.ngain), onepass_bytes(dk, prep.ngain), "one-pass sweep"
+    elif e_ms >= h_ms:
+        dom_ms, dom_b, dom_b2, dom = e_ms, eb, eb2, "E sweep"
+    else:
+        dom_ms, dom_b, dom_b2, dom = h_ms, hb, hb2, "H sweep"
+    ach = dom_b / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    ach2 = dom_b2 / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    step_b = (hb + eb) / prep.cells
+    roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": P["hbm_gbs"], "unit": "GB/s",
+            "frac": ach / P["hbm_gbs"], "peak_source": src, "traffic": None,
+            "algorithmic_bytes_per_launch": dom_b,
+            "byte_model": "swept side's fields read+written once + 1 B ID + psi + aux state (other side not counted)",
+            "two_sweep_bytes_per_launch": dom_b2, "achieved_two_sweep": ach2, "frac_two_sweep": ach2 / P["hbm_gbs"],
+            "launch_ms": dom_ms, "samples": nsamp,
+            "launch_timing": "CUDA events around each sweep on the grid's stream, 200 more time steps after the "
+                             "timed region",
+            "h_sweep_ms": h_ms, "e_sweep_ms": e_ms,
+            "h_sweep_frac": hb / (h_ms / 1e3) / 1e9 / P["hbm_gbs"] if h_ms else 0,
+            "step_bytes_per_cell": step_b,
+            "step_frac": value_per_gpu * step_b / P["hbm_gbs"]}
+    tr = os.path.join(ROOT, "profiles", "traffic.json")
+    key = f"{prep.kind}_{dk.nx}_{'onepass' if path == cps.ONEPASS else 'fused'}"
+    if os.path.exists(tr):
+        try:
+            t = json.load(open(tr)).get(key)
+            if t:
+                roof["traffic"] = t["e_sweep_bytes_per_launch"] if dom == "E sweep" else t.get("h_sweep_bytes_per_launch")
+                roof["traffic_source"] = t["source"]
+        except (ValueError, OSError, KeyError):
+            pass
+    return roof
+
+
+def e2e_jobs(prep, prec, path, jobs, local, dist, steps=None):
+    """Whole jobs through the C ABI from host buffers: grid set-up from the
+    deck with the IDs and port points in pinned host memory, `steps` time
+    steps (the job's own count by default), the port spectra read back into
+    pinned host buffers allocated once, teardown."""
+    import torch
+    dk = prep.dk
+    steps = steps or dk.nsteps
+    pinned_ids = torch.from_numpy(np.ascontiguousarray(prep.ids)).pin_memory()
+    pinned_out = [torch.empty(len(pp) * bin(p.dft_mask).count("1") * len(p.dft_freqs) * 2, dtype=torch.float64)
+                  .pin_memory().numpy() if p.dft_freqs is not None else None for p, pp in zip(dk.ports, prep.pts)]
+    outs = []
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(jobs):
+        gg = prep.grid(prec, local, ids=pinned_ids.numpy())
+        gg.step(steps, path)
+        outs = [gg.port_dft(n, raw=True, out=pinned_out[n]) for n in range(len(dk.ports))
+                if pinned_out[n] is not None]
+        gg.close()
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([t], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    world = dist.get_world_size() if dist else 1
+    h2d = prep.ids.nbytes + sum(p.nbytes for p in prep.pts) + sum(len(w) * 8 for *_, w in dk.sources)
+    d2h = sum(o.nbytes for o in outs)
+    return {"value": prep.cells * steps * jobs * world / t / 1e9, "unit": "Gcell-upd/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "job_time_steps": steps, "seconds": t}
+
+
+def fp64_legs(prep, args, local, dist):
+    """The deck in FP64: the plain path (one kernel per reference routine, the
+    form the oracle pins) and the fused path, each over args.fp64_chunks
+    bench steps after one warm-up; e2e on the plain path over a job of
+    args.fp64_e2e_steps time steps."""
+    import cpsfdtd_b200 as cps
+    out = {}
+    for name, path in (("plain", cps.PLAIN), ("fused", cps.FUSED)):
+        g = prep.grid(cps.FP64, local)
+        st = Stepper(g, prep.dk, args.chunk, path)
+        ms, nts, launches, _ = timed_chunks(g, st, 1, args.fp64_chunks, dist)
+        v, ms = aggregate(prep.cells * nts, ms, dist, f"cuda:{local}")
+        out[name] = {"value": v / 1e9, "unit": "Gcell-upd/s", "ms_per_step": ms / args.fp64_chunks,
+                     "steps": args.fp64_chunks, "time_steps_per_step": args.chunk, "gpu_launches": int(launches)}
+        g.close()
+    out["e2e_plain"] = e2e_jobs(prep, cps.FP64, cps.PLAIN, 1, local, dist,
+                                steps=min(args.fp64_e2e_steps, prep.dk.nsteps))
+    out["dtype"] = "f64"
+    return out
+
+
+def grid_report(a, b, dk):
+    """accuracy of grid a against grid b: fields and every DFT port"""
+    from cpsfdtd_b200 import accuracy
+    ports = [accuracy.port_errors(p.dft_freqs, a.port_dft(n, raw=True), b.port_dft(n, raw=True))
+             for n, p in enumerate(dk.ports) if p.dft_freqs is not None]
+    return accuracy.summarize(accuracy.field_errors([a.field(c) for c in range(6)], [b.field(c) for c in range(6)]),
+                              ports)
+
+
+def accuracy_legs(args, local, c3_prep, c2_prep):
+    """Per config, the chosen FP32 forms against FP64 runs of the same decks:
+    C1 (96^3, 1000 steps), C2 (256^3, 4000 steps) and C3 (384^3, the first
+    args.acc_c3_steps steps) fused FP32 against FP64; C4, one 128^3 member
+    batched with two others for its 5000 steps against it alone in FP64.  The
+    FP64 side is the fused FP64 path, checked here against the plain FP64
+    path (which equals the oracle bit for bit on C1)."""
+    import cpsfdtd_b200 as cps
+    from cpsfdtd_b200 import decks
+    rep = {"reference": "FP64 fused path on the GPU (agreement with the FP64 plain path reported as "
+                        "fp64_fused_vs_plain; the plain path equals the oracle bit for bit on C1 at 96^3 x 1000)"}
+    c1 = decks.config1(n=96, steps=1000)
+    cases = [("c1", c1, cps.rasterize(c1.nx, c1.ny, c1.nz, c1.dx, c1.dy, c1.dz, c1.shapes),
+              [cps.port_points(c1, p) for p in c1.ports], c1.nsteps)]
+    if c2_prep is not None:
+        cases.append(("c2", c2_prep.dk, c2_prep.ids, c2_prep.pts, c2_prep.dk.nsteps))
+    if c3_prep is not None:
+        cases.append(("c3", c3_prep.dk, c3_prep.ids, c3_prep.pts, min(args.acc_c3_steps, c3_prep.dk.nsteps)))
+    for name, dk, ids, pts, steps in cases:
+
+        def run(prec, path):
+            g = cps.Grid.from_deck(dk, prec, ids=ids, port_points_list=pts, device=local)
+            g.step(steps, path)
+            g.sync()
+            return g
+
+        f64 = run(cps.FP64, cps.FUSED)
+        p64 = run(cps.FP64, cps.PLAIN)
+        r64 = grid_report(f64, p64, dk)
+        p64.close()
+        f32 = run(cps.FP32, cps.FUSED)
+        r = grid_report(f32, f64, dk)
+        r["time_steps"] = steps
+        r["grid"] = [dk.nx, dk.ny, dk.nz]
+        r["form"] = "fp32 fused, one grid"
+        r["fp64_fused_vs_plain_field_rel_l2"] = r64["field_rel_l2"]
+        if dk.gain:
+            r["population_max_abs_err"] = float(np.abs(f32.populations() - f64.populations()).max())
+        f32.close()
+        f64.close()
+        rep[name] = r
+    # C4: a member inside a batch
+    dks = [decks.config4_member(128, 128, 128, seed=7, steps=5000, nfreq=32),
+           decks.config4_member(64, 96, 80, seed=8, steps=5000, nfreq=32),
+           decks.config4_member(112, 64, 128, seed=9, steps=5000, nfreq=32)]
+    b = cps.Batch(cps.FP32)
+    gs = [cps.Grid.from_deck(d, cps.FP32, device=local) for d in dks]
+    for g in gs:
+        b.add(g)
+    b.step(5000)
+    b.sync()
+    ref = cps.Grid.from_deck(dks[0], cps.FP64, device=local)
+    ref.step(5000, cps.FUSED)
+    ref.sync()
+    r = grid_report(gs[0], ref, dks[0])
+    r.update({"time_steps": 5000, "grid": [128, 128, 128], "form": "fp32 batched (3 members) vs fp64 alone"})
+    rep["c4"] = r
+    b.close()
+    for g in gs + [ref]:
+        g.close()
+    return rep
 
 
 def ensemble(args, local, dist):
@@ -319,18 +605,30 @@ def ensemble(args, local, dist):
     tile = list(b.get_tile())
     b.close()
 
-    def loop(path):
+    def loop(path, steps):
+        # one grid after another on the device: each grid's stream waits for
+        # the previous grid's last launch; events on the current stream bracket
+        # the chain
+        cur = torch.cuda.current_stream(local)
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        ts = time.perf_counter()
+        s0.record(cur)
+        prev = s0
         for g in grids:
-            g.step(args.ens_loop_steps, path)
-            g.sync()
-        torch.cuda.synchronize()
-        return cells * args.ens_loop_steps / (time.perf_counter() - ts) / 1e9
+            gs = torch.cuda.ExternalStream(g.stream(), device=local)
+            gs.wait_event(prev)
+            g.step(steps, path)
+            prev = torch.cuda.Event()
+            prev.record(gs)
+        cur.wait_event(prev)
+        s1.record(cur)
+        s1.synchronize()
+        return cells * steps / (s0.elapsed_time(s1) / 1e3) / 1e9
 
-    loop(cps.FUSED)  # warm-up of the one-grid kernels
-    plain = loop(cps.PLAIN)
-    fused = loop(cps.FUSED)
+    loop(cps.FUSED, 2)  # warm-up of the one-grid kernels
+    plain = loop(cps.PLAIN, args.ens_loop_steps)
+    fused = loop(cps.FUSED, args.ens_loop_steps)
     for g in grids:
         g.close()
     return {"workload": f"{args.ens_grids} disordered-crystal realizations, edges U{{64,80,96,112,128}} per axis, "
@@ -342,7 +640,8 @@ def ensemble(args, local, dist):
             "speedup_vs_fused_loop": batched / fused if fused else None,
             "gpu_launches": int(launches), "setup_s": setup_s, "autotune_s": tune_s,
             "autotune_steps": tuned_steps, "loop_steps_per_grid": args.ens_loop_steps,
-            "timing": "batched: CUDA events on the batch stream; loops: host clock with a device sync per grid"}
+            "timing": "all arms: CUDA events around the whole loop on the device (the loops' grids stepped one "
+                      "after another, each grid's stream waiting for the previous grid's last launch)"}
 
 
 def serve_jobs(count, step_scale, seed=0):
@@ -377,9 +676,12 @@ def serving(args, local):
     """Served job stream through the library's serving loop (Poisson arrivals
     offered at --serve-load times a 20 Gcell-upd/s service rate, admission
     against a 180 GB budget, continuous batching), against the same jobs run
-    one at a time on the plain per-routine GPU path, queued in arrival order."""
+    one at a time on the plain per-routine GPU path, queued in arrival order.
+    Accuracy: the smallest job of each material kind, served in FP32, against
+    the same deck run alone in FP64."""
     import torch
     import cpsfdtd_b200 as cps
+    from cpsfdtd_b200 import accuracy
     jobs = serve_jobs(args.serve_jobs, args.serve_step_scale)
     work = [e ** 3 * st for _, e, st, _ in jobs]
     rng = np.random.Generator(np.random.PCG64(1))
@@ -391,6 +693,13 @@ def serving(args, local):
     budget = min(budget, int(free * 0.9))
     tile = tuple(int(v) for v in args.serve_tile.split(",")) if args.serve_tile else None
     srv = cps.Server(cps.FP32, max_jobs=256, budget_bytes=budget, chunk_steps=64, tile=tile)
+    # the smallest job of each material kind is checked against an FP64 run alone
+    checked = {}
+    for n, (kind, edge, steps, seed) in enumerate(jobs):
+        if kind not in checked or edge ** 3 * steps < jobs[checked[kind]][1] ** 3 * jobs[checked[kind]][2]:
+            checked[kind] = n
+    check_ids = set(checked.values())
+    kept = {}
     done = {}
     t0 = time.perf_counter()
     nxt = 0
@@ -402,9 +711,9 @@ def serving(args, local):
 
             def fin(g, status, n=nxt):
                 if g is not None and status == 0:
-                    for p in range(len(g.ports)):
-                        if g.ports[p][2] > 0:
-                            g.port_dft(p, raw=True)
+                    dfts = [g.port_dft(p, raw=True) for p in range(len(g.ports)) if g.ports[p][2] > 0]
+                    if n in check_ids:
+                        kept[n] = ([g.field(c) for c in range(6)], dfts)
                 done[n] = (status, time.perf_counter() - t0)
 
             srv.submit(lambda dk=dk: cps.Grid.from_deck(dk, cps.FP32, device=local), fin, steps,
@@ -438,6 +747,29 @@ def serving(args, local):
         finish = max(finish, a) + sv
         plain_lat.append(finish - a)
     plain_lat.sort()
+
+    # accuracy of the served results against FP64 runs alone
+    acc = {}
+    for kind, n in sorted(checked.items()):
+        if n not in kept:
+            continue
+        _, edge, steps, seed = jobs[n]
+        dk = serve_deck(kind, edge, steps, seed)
+        g = cps.Grid.from_deck(dk, cps.FP64, device=local)
+        g.step(steps, cps.FUSED)
+        g.sync()
+        fields, dfts = kept[n]
+        ports = []
+        k = 0
+        for p_i, p in enumerate(dk.ports):
+            if p.dft_freqs is not None:
+                ports.append(accuracy.port_errors(p.dft_freqs, dfts[k], g.port_dft(p_i, raw=True)))
+                k += 1
+        r = accuracy.summarize(accuracy.field_errors(fields, [g.field(c) for c in range(6)]), ports)
+        r.update({"job": n, "grid": [edge] * 3, "time_steps": steps, "form": "fp32 served vs fp64 alone"})
+        acc[kind] = r
+        g.close()
+
     pct = lambda v, q: float(np.percentile(v, q))
     return {"workload": f"{len(jobs)} jobs, edge log-uniform [48,320], steps log-uniform [500,20000]/"
                         f"{args.serve_step_scale:g}, mix 40% dielectric / 35% Drude-Lorentz+TF/SF / 25% gain; "
@@ -453,146 +785,92 @@ def serving(args, local):
                                     "gcell_upd_per_s": cells_total / sum(service) / 1e9,
                                     "latency_p50_s": pct(plain_lat, 50), "latency_p99_s": pct(plain_lat, 99)},
             "speedup_gcell_vs_plain": (cells_total / span) / (cells_total / sum(service)),
+            "accuracy": acc,
             "timing": "host clock: job latency = completion - arrival, including deck generation and grid "
                       "set-up; plain latencies from measured service times queued in arrival order"}
+
+
+def headline(prep, args, local, dist, clocks_on=True):
+    """FP32 value, roofline and e2e of one deck."""
+    import cpsfdtd_b200 as cps
+    import torch
+    path = cps.ONEPASS if args.path == "onepass" else cps.FUSED
+    g = prep.grid(cps.FP32, local)
+    st = Stepper(g, prep.dk, args.chunk, path)
+    clocks = Clocks(local) if clocks_on else None
+    ms, nts, launches, clk = timed_chunks(g, st, args.warmup, args.steps, dist, clocks)
+    value, ms = aggregate(prep.cells * nts, ms, dist, f"cuda:{local}")
+    value /= 1e9
+    world = dist.get_world_size() if dist else 1
+    roof = sweep_roofline(prep, g, path, value / world)
+    g.close()
+    torch.cuda.synchronize()
+    e2e = e2e_jobs(prep, cps.FP32, path, args.e2e_jobs, local, dist) if args.e2e_jobs > 0 else None
+    return {"value": value, "ms_per_step": ms / args.steps, "time_steps_timed": nts, "gpu_launches": int(launches),
+            "roofline": roof, "clocks": clk, "e2e": e2e}
+
+
+def c2_leg(prep, args, local, dist):
+    """The dispersive-scattering deck beside the headline: whole 4000-step
+    jobs (one warm-up, args.c2_jobs timed), roofline, e2e, FP64 legs."""
+    a = argparse.Namespace(**vars(args))
+    a.chunk, a.warmup, a.steps = prep.dk.nsteps, 1, args.c2_jobs
+    h = headline(prep, a, local, dist, clocks_on=False)
+    out = {"workload": workload_name(prep.dk, "dispersive", a.chunk), "grid": [prep.dk.nx] * 3,
+           "metric": "Gcell-upd/s", "value": h["value"], "ms_per_step": h["ms_per_step"], "steps": a.steps,
+           "roofline": h["roofline"], "e2e": h["e2e"], "gpu_launches": h["gpu_launches"], "dtype": "fp32"}
+    if not args.no_fp64:
+        a.fp64_chunks = 1
+        a.fp64_e2e_steps = prep.dk.nsteps
+        out["fp64"] = fp64_legs(prep, a, local, dist)
+    return out
 
 
 def run_ours(args):
     import torch
     world, rank, local, dist = dist_setup()
-    import cpsfdtd_b200 as cps
+    import cpsfdtd_b200 as cps  # noqa: F401
     torch.cuda.set_device(local)
-    dk = workload(args.n, args.job_steps, args.workload)
-    ids = _ids(dk)
-    pts = [cps.port_points(dk, p) for p in dk.ports]
-    g = cps.Grid.from_deck(dk, cps.FP32, ids=ids, port_points_list=pts, device=local)
-    stream = torch.cuda.ExternalStream(g.stream(), device=local)
-
-    path = cps.ONEPASS if args.path == "onepass" else cps.FUSED
-
-    def job(grid):
-        grid.reset(dk.n0)
-        grid.step(dk.nsteps, path)
-        grid.flush_ports()
-
-    for _ in range(args.warmup):
-        job(g)
-    g.sync()
-    launches0 = g.launches()
-    clocks = Clocks(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        job(g)
-    e1.record(stream)
-    e1.synchronize()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    launches = g.launches() - launches0
-    # the sweeps' own durations: per-step CUDA events on one more job, stepped
-    # as the direct launch sequence (the timed jobs replay the same kernels in
-    # CUDA-graph chunks, where single launches are not timed)
-    g.set_timing(1)
-    job(g)
-    g.sync()
-    h_ms, e_ms, nsamp = g.timing()
-    g.set_timing(0)
-    cells = dk.cells
-    value, ms = aggregate(cells * dk.nsteps * args.steps, ms, dist, f"cuda:{local}")
-    value /= 1e9
-
-    # roofline of the dominant kernel (E sweep)
-    P, src = peaks()
-    ndl = 0
-    from cpsfdtd_b200 import decks
-    ndl = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_DISPERSIVE).sum()) if dk.dl else 0
-    ngain = int(((ids[1:-1, 1:-1, 1:-1]) == decks.ID_GAIN).sum()) if dk.gain else 0
-    hb, eb = sweep_bytes(dk, ndl, ngain=ngain)
-    if path == cps.ONEPASS:  # h_ms: the one-pass sweep (with its TF/SF terms); e_ms: the Drude-Lorentz cells
-        dom_ms, dom_bytes, dom = h_ms, onepass_bytes(dk, ngain), "one-pass sweep"
-    else:
-        dom_ms, dom_bytes, dom = (e_ms, eb, "E sweep") if e_ms >= h_ms else (h_ms, hb, "H sweep")
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": P["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / P["hbm_gbs"], "peak_source": src, "traffic": None,
-            "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": dom_ms, "samples": nsamp,
-            "launch_timing": "CUDA events around each sweep on the grid's stream, one job after the timed region",
-            "h_sweep_ms": h_ms, "e_sweep_ms": e_ms,
-            "step_bytes_per_cell": (hb + eb) / cells,
-            "step_frac_at_50B": value / world * 50 / P["hbm_gbs"]}
-    tr = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tr) and args.workload == "dispersive" and args.n == 256 and path == cps.FUSED:
+    prep = Prepared(args.workload, args.n, args.job_steps)
+    h = headline(prep, args, local, dist)
+    fp64 = None if args.no_fp64 else fp64_legs(prep, args, local, dist)
+    c2 = None
+    c2_prep = None
+    if args.workload == "laser" and not args.no_c2:
+        c2_prep = Prepared("dispersive", 256, 4000)
+        c2 = c2_leg(c2_prep, args, local, dist)
+    acc = None
+    if not args.no_accuracy and world == 1:
         try:
-            roof["traffic"] = json.load(open(tr)).get("e_sweep_bytes_per_launch")
-        except (ValueError, OSError):
-            pass
-
-    # end to end through the C ABI from host buffers
-    e2e = None
-    if args.e2e_steps > 0:
-        pinned_ids = torch.from_numpy(np.ascontiguousarray(ids)).pin_memory()
-        # spectra land in pinned host buffers allocated once, like the inputs
-        pinned_out = [torch.empty(len(pp) * bin(p.dft_mask).count("1") * len(p.dft_freqs) * 2, dtype=torch.float64)
-                      .pin_memory().numpy() if p.dft_freqs is not None else None for p, pp in zip(dk.ports, pts)]
-        outs = []
-        h2d = d2h = 0
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.e2e_steps):
-            gg = cps.Grid.from_deck(dk, cps.FP32, ids=pinned_ids.numpy(), port_points_list=pts, device=local)
-            gg.step(dk.nsteps, path)
-            outs = [gg.port_dft(n, raw=True, out=pinned_out[n]) for n in range(len(dk.ports))
-                    if pinned_out[n] is not None]
-            gg.close()
-        torch.cuda.synchronize()
-        t_e2e = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([t_e2e], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_e2e = float(t.item())
-        h2d = ids.nbytes + sum(p.nbytes for p in pts) + sum(len(w) * 8 for *_, w in dk.sources)
-        d2h = sum(o.nbytes for o in outs)
-        e2e = {"value": cells * dk.nsteps * args.e2e_steps * world / t_e2e / 1e9, "unit": "Gcell-upd/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
-
+            acc = accuracy_legs(args, local, prep if args.workload == "laser" else None,
+                                c2_prep if args.workload == "laser" else prep)
+        except Exception as ex:
+            acc = {"error": str(ex)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        try:
-            cpu = cpu_baseline(workload(args.n, args.job_steps, args.workload), args.cpu_steps, args.workload)
-        except Exception as ex:  # the baseline is reported, never required
-            cpu = {"value": None, "unit": "Gcell-upd/s", "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"failed: {ex}"}
-    srv = None
-    if args.serve_jobs > 0 and world == 1:
-        try:
-            srv = serving(args, local)
-        except Exception as ex:
-            srv = {"error": str(ex)}
+        cpu = cpu_baseline(prep, args.cpu_steps)
     ens = None
     if args.ens_grids > 0:
         try:
             ens = ensemble(args, local, dist)
         except Exception as ex:
             ens = {"error": str(ex)}
+    srv = None
+    if args.serve_jobs > 0 and world == 1:
+        try:
+            srv = serving(args, local)
+        except Exception as ex:
+            srv = {"error": str(ex)}
     if rank == 0:
-        line = {"metric": "Gcell-upd/s", "value": value, "unit": "Gcell-upd/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        line = {"metric": "Gcell-upd/s", "value": h["value"], "unit": "Gcell-upd/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": h["ms_per_step"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
                 "data": "synthetic (seeded deck generator)",
-                "config": config_of(dk, args.workload, world, args.path),
-                "roofline": roof, "clocks": clk, "gpu_launches": int(launches),
-                "e2e": e2e, "cpu_baseline": cpu, "ensemble": ens, "serving": srv}
+                "config": config_of(prep.dk, args.workload, world, args.chunk, args.path),
+                "roofline": h["roofline"], "clocks": h["clocks"], "gpu_launches": h["gpu_launches"],
+                "e2e": h["e2e"], "fp64": fp64, "c2": c2, "accuracy": acc, "cpu_baseline": cpu,
+                "ensemble": ens, "serving": srv}
         print(json.dumps(line), flush=True)
-    g.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

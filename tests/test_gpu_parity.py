@@ -44,6 +44,9 @@ def _c3_three():
 
 
 CASES = {"c1": lambda: decks.config1(n=32, steps=120),
+         # the reference's own CPML coefficients (literal) in an eps 2.25 CPML,
+         # before that form starts to diverge
+         "c3_literal_pml": lambda: gc.literal_pml(decks.config3(n=40, steps=100, nfreq=4)),
          "c2_drude": _c2_drude,
          "c3_three": _c3_three,
          "c2": lambda: decks.config2(n=48, steps=100, nfreq=8),
