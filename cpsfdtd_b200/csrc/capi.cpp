@@ -1148,6 +1148,10 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     G.r_t21_2 = 1.0 / G.t21_2; G.r_t32_2 = 1.0 / G.t32_2;
     G.r_hwb = 1.0 / G.homega_bdt; G.r_hwa = 1.0 / G.homega_adt;
     G.inv_scale = 1.0 / G.scaleP;
+    G.k1a = (float)(dt / (2.0 * p->t21)); G.k1b = (float)(dt / (2.0 * p->t10));
+    G.k3a = (float)(dt / (2.0 * p->t32)); G.k3b = (float)(dt / (2.0 * p->t30));
+    G.ha = (float)(dt / (2.0 * G.homega_adt) * G.inv_scale); G.hb = (float)(dt / (2.0 * G.homega_bdt) * G.inv_scale);
+    G.fpump = (float)G.pump_dt;
     g->gain_id = p->gain_id;
     if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg, &g->d_g_segm))) return s;
     const int nw = g->fp32 ? kG32Words : kG64Words;

@@ -95,32 +95,49 @@ struct GainSite32 {
     static constexpr int PA = 0, PA1 = 3, PB = 6, PB1 = 9, DN1 = 12, N2 = 13, N3 = 14, PA2 = 15, PB2 = 18, E1 = 21;
 };
 
-// populations of a site as FP64 N0..N3
+// Populations of a site.  FP64 grids keep N0..N3 as the reference does.
+// FP32 grids keep the offsets from the initial state, n1 = N1 - 1, n2 = N2,
+// n3 = N3, and m0 = N0 - 1 = -(n1 + n2 + n3) from conservation (the sum in
+// FP64, FourLevelLaser.cpp:324), so no update subtracts numbers near 1.
 template <typename T>
-__device__ __forceinline__ void gain_load_n(const T *st, int64_t sc, double N[4]);
+struct Pops {
+    double N[4];
+};
 template <>
-__device__ __forceinline__ void gain_load_n<double>(const double *st, int64_t sc, double N[4])
+struct Pops<float> {
+    float n1, n2, n3, m0;
+};
+
+__device__ __forceinline__ float conserve_m0(float n1, float n2, float n3)
 {
-    for (int q = 0; q < 4; ++q) N[q] = st[(GainSite64::N + q) * sc];
+    return (float)(-((double)n1 + (double)n2 + (double)n3));
+}
+
+template <typename T>
+__device__ __forceinline__ void gain_load_n(const T *st, int64_t sc, Pops<T> &P);
+template <>
+__device__ __forceinline__ void gain_load_n<double>(const double *st, int64_t sc, Pops<double> &P)
+{
+    for (int q = 0; q < 4; ++q) P.N[q] = st[(GainSite64::N + q) * sc];
 }
 template <>
-__device__ __forceinline__ void gain_load_n<float>(const float *st, int64_t sc, double N[4])
+__device__ __forceinline__ void gain_load_n<float>(const float *st, int64_t sc, Pops<float> &P)
 {
-    N[1] = 1.0 + (double)st[GainSite32::DN1 * sc];
-    N[2] = (double)st[GainSite32::N2 * sc];
-    N[3] = (double)st[GainSite32::N3 * sc];
-    N[0] = 2.0 - N[1] - N[2] - N[3];  // FP64 conservation, FourLevelLaser.cpp:324
+    P.n1 = st[GainSite32::DN1 * sc];
+    P.n2 = st[GainSite32::N2 * sc];
+    P.n3 = st[GainSite32::N3 * sc];
+    P.m0 = conserve_m0(P.n1, P.n2, P.n3);
 }
 
 // P update (FourLevelLaser.cpp:274-295) with explicit P, P1 in/out and the
 // shifted-out P2 returned; P values are in the grid's storage scale.
 template <typename T>
-__device__ __forceinline__ void gain_p_update(const GainCoef &G, const double N[4], const T E[3], T Pa[3],
+__device__ __forceinline__ void gain_p_update(const GainCoef &G, const Pops<T> &P, const T E[3], T Pa[3],
                                               T Pa1[3], T Pa2[3], T Pb[3], T Pb1[3], T Pb2[3])
 {
     const T ca1 = (T)G.CPa1, ca2 = (T)G.CPa2, ca3 = (T)(G.CPa3 * G.scaleP);
     const T cb1 = (T)G.CPb1, cb2 = (T)G.CPb2, cb3 = (T)(G.CPb3 * G.scaleP);
-    const T dNa = (T)(N[2] - N[1]), dNb = (T)(N[3] - N[0]);
+    const T dNa = (T)(P.N[2] - P.N[1]), dNb = (T)(P.N[3] - P.N[0]);
     for (int c = 0; c < 3; ++c) {
         Pa2[c] = Pa1[c];
         Pa1[c] = Pa[c];
@@ -134,13 +151,13 @@ __device__ __forceinline__ void gain_p_update(const GainCoef &G, const double N[
 }
 
 // FP32 grids: the same recursion with the float coefficients prepared on the
-// host (bit-identical to converting them here)
+// host; N2 - N1 = (n2 - n1) - 1 and N3 - N0 = (n3 - m0) - 1
 template <>
-__device__ __forceinline__ void gain_p_update<float>(const GainCoef &G, const double N[4], const float E[3],
+__device__ __forceinline__ void gain_p_update<float>(const GainCoef &G, const Pops<float> &P, const float E[3],
                                                      float Pa[3], float Pa1[3], float Pa2[3], float Pb[3],
                                                      float Pb1[3], float Pb2[3])
 {
-    const float dNa = (float)(N[2] - N[1]), dNb = (float)(N[3] - N[0]);
+    const float dNa = (P.n2 - P.n1) - 1.0f, dNb = (P.n3 - P.m0) - 1.0f;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         Pa2[c] = Pa1[c];
@@ -167,10 +184,11 @@ __device__ __forceinline__ T gain_e_corr(const GainCoef &G, T E, T pa, T pa1, T 
 // uses Pay - Pay_1 as the reference does (:316), Ez follows the Ex form; the
 // pump moves pump_rate*dt*N0 from N0 to N3.
 template <typename T>
-__device__ __forceinline__ void gain_n_update(const GainCoef &G, double N[4], const T E[3], const T E1[3],
+__device__ __forceinline__ void gain_n_update(const GainCoef &G, Pops<T> &P, const T E[3], const T E1[3],
                                               const T Pa[3], const T Pa1[3], const T Pa2[3], const T Pb[3],
                                               const T Pb2[3])
 {
+    double *N = P.N;
     const double inv = 1.0 / G.scaleP;
     // on FP64 grids (scaleP == 1) the sums keep the reference's exact roundings
     double sb = (double)E1[0] * ((double)Pb[0] - (double)Pb2[0]) + (double)E1[1] * ((double)Pb[1] - (double)Pb2[1]);
@@ -192,43 +210,54 @@ __device__ __forceinline__ void gain_n_update(const GainCoef &G, double N[4], co
     N[0] = 2.0 - N[1] - N[2] - N[3];
 }
 
-// FP32 grids: the energy-exchange sums E.(P - P'') are formed in float (P
-// carries the factor CEP), the populations stay FP64 with the constant
-// divisors applied as host-computed reciprocals; N0 from conservation in FP64.
+// FP32 grids: the same semi-implicit update in FP32 on the offsets.  Dividing
+// numerator and denominator of each update by its lifetime product (2 t30 t32,
+// 2 t10 t21, 2 t32 t21) and writing N1 = 1 + n1, N0 = 1 + m0 gives, with
+// k1a = dt/2t21, k1b = dt/2t10, k3a = dt/2t32, k3b = dt/2t30, ha = dt/2hwa,
+// hb = dt/2hwb (hw* = homega_*dt; ha, hb also undo P's storage scale):
+//   n3' = [n3 (1 + k3b m0 - k3a (1 - n2)) + hb sb] / [1 + k3a (1 - n2) - k3b m0]
+//         + pump dt (1 + m0)
+//   n1' = [n1 (1 + k1b m0 - k1a n2) + 2 k1b m0 - ha sa] / [1 + k1a n2 - k1b m0]
+//   n2' = [n2 (1 + k1a n1' - k3a n3') + 2 k3a n3' + ha s2] / [1 + k3a n3' - k1a n1']
+// (algebraically the reference's expressions; every term is an offset or a
+// small multiple of one, so FP32 keeps the offsets to a few ulps), then
+// m0' = -(n1' + n2' + n3') in FP64.  The energy-exchange sums E.(P - P'') are
+// formed in float.
 template <>
-__device__ __forceinline__ void gain_n_update<float>(const GainCoef &G, double N[4], const float E[3],
+__device__ __forceinline__ void gain_n_update<float>(const GainCoef &G, Pops<float> &P, const float E[3],
                                                      const float E1[3], const float Pa[3], const float Pa1[3],
                                                      const float Pa2[3], const float Pb[3], const float Pb2[3])
 {
-    const float fsb = E1[0] * (Pb[0] - Pb2[0]) + E1[1] * (Pb[1] - Pb2[1]) + E1[2] * (Pb[2] - Pb2[2]);
-    const float fsa = E1[0] * (Pa[0] - Pa2[0]) + E1[1] * (Pa[1] - Pa2[1]) + E1[2] * (Pa[2] - Pa2[2]);
-    const float fs2 = (E[0] + E1[0]) * (Pa[0] - Pa2[0]) + (E[1] + E1[1]) * (Pa[1] - Pa1[1]) +
-                      (E[2] + E1[2]) * (Pa[2] - Pa2[2]);
-    const double sb = (double)fsb * G.inv_scale, sa = (double)fsa * G.inv_scale, s2 = (double)fs2 * G.inv_scale;
-    const double N0old = N[0];
-    N[3] = G.t30t32dt / (G.t30t32_2 + G.t30dt * (1 - N[2]) + G.t32dt * (1 - N[0])) *
-           (N[3] * ((N[0] - 1) * G.r_t30 + (N[2] - 1) * G.r_t32 + G.dt_2) + sb * G.r_hwb);
-    N[3] = N[3] + G.pump_dt * N0old;
-    N[1] = G.t10t21dt / (G.t10t21_2 + G.t10dt * N[2] + G.t21dt * (1 - N[0])) *
-           (N[1] * ((N[0] - 1) * G.r_t10 - N[2] * G.r_t21 + G.dt_2) + N[2] * G.r_t21_2 - sa * G.r_hwa);
-    N[2] = G.t32t21dt / (G.t32t21_2 + G.t21dt * N[3] + G.t32dt * (1 - N[1])) *
-           (N[2] * ((N[1] - 1) * G.r_t21 - N[3] * G.r_t32 + G.dt_2) + N[3] * G.r_t32_2 + s2 * G.r_hwa);
-    N[0] = 2.0 - N[1] - N[2] - N[3];
+    const float sb = E1[0] * (Pb[0] - Pb2[0]) + E1[1] * (Pb[1] - Pb2[1]) + E1[2] * (Pb[2] - Pb2[2]);
+    const float sa = E1[0] * (Pa[0] - Pa2[0]) + E1[1] * (Pa[1] - Pa2[1]) + E1[2] * (Pa[2] - Pa2[2]);
+    const float s2 = (E[0] + E1[0]) * (Pa[0] - Pa2[0]) + (E[1] + E1[1]) * (Pa[1] - Pa1[1]) +
+                     (E[2] + E1[2]) * (Pa[2] - Pa2[2]);
+    const float n1 = P.n1, n2 = P.n2, n3 = P.n3, m0 = P.m0;
+    const float q3 = G.k3a * (1.0f - n2) - G.k3b * m0;
+    const float n3n = __fdividef(n3 * (1.0f - q3) + G.hb * sb, 1.0f + q3) + G.fpump * (1.0f + m0);
+    const float q1 = G.k1a * n2 - G.k1b * m0;
+    const float n1n = __fdividef(n1 * (1.0f - q1) + 2.0f * G.k1b * m0 - G.ha * sa, 1.0f + q1);
+    const float q2 = G.k3a * n3n - G.k1a * n1n;
+    const float n2n = __fdividef(n2 * (1.0f - q2) + 2.0f * G.k3a * n3n + G.ha * s2, 1.0f + q2);
+    P.n1 = n1n;
+    P.n2 = n2n;
+    P.n3 = n3n;
+    P.m0 = conserve_m0(n1n, n2n, n3n);
 }
 
 template <typename T>
-__device__ __forceinline__ void gain_store_n(T *st, int64_t sc, const double N[4]);
+__device__ __forceinline__ void gain_store_n(T *st, int64_t sc, const Pops<T> &P);
 template <>
-__device__ __forceinline__ void gain_store_n<double>(double *st, int64_t sc, const double N[4])
+__device__ __forceinline__ void gain_store_n<double>(double *st, int64_t sc, const Pops<double> &P)
 {
-    for (int q = 0; q < 4; ++q) st[(GainSite64::N + q) * sc] = N[q];
+    for (int q = 0; q < 4; ++q) st[(GainSite64::N + q) * sc] = P.N[q];
 }
 template <>
-__device__ __forceinline__ void gain_store_n<float>(float *st, int64_t sc, const double N[4])
+__device__ __forceinline__ void gain_store_n<float>(float *st, int64_t sc, const Pops<float> &P)
 {
-    st[GainSite32::DN1 * sc] = (float)(N[1] - 1.0);
-    st[GainSite32::N2 * sc] = (float)N[2];
-    st[GainSite32::N3 * sc] = (float)N[3];
+    st[GainSite32::DN1 * sc] = P.n1;
+    st[GainSite32::N2 * sc] = P.n2;
+    st[GainSite32::N3 * sc] = P.n3;
 }
 
 // TF/SF incident-table lookup, TF_SF.cpp:966-986; indices past the table read 0

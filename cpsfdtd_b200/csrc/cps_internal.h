@@ -74,6 +74,10 @@ struct GainCoef {
     // constant divisors of the population update as FP64 reciprocals
     float fa1, fa2, fa3, fb1, fb2, fb3;
     double r_t30, r_t32, r_t21, r_t10, r_t21_2, r_t32_2, r_hwb, r_hwa, inv_scale;
+    // FP32 grids: the population update on offsets (cells.cuh gain_n_update<float>):
+    // k1a = dt/2t21, k1b = dt/2t10, k3a = dt/2t32, k3b = dt/2t30,
+    // ha = dt/(2 homega_adt)/scaleP, hb = dt/(2 homega_bdt)/scaleP, fpump = pump_rate dt
+    float k1a, k1b, k3a, k3b, ha, hb, fpump;
 };
 
 // per-cell gain state words

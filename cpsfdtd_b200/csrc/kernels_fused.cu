@@ -244,7 +244,7 @@ k_e_fused(FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc)
                     T *st = G.state + c;
                     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
                     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
-                    double N[4];
+                    Pops<T> N;
                     if (sizeof(T) == 8) {
                         using L = GainSite64;
 #pragma unroll

@@ -188,7 +188,7 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
         Pb[q] = st[(L::PB + q) * sc]; Pb1[q] = st[(L::PB1 + q) * sc];
     }
     if (which == 0) {
-        double N[4];
+        Pops<T> N;
         gain_load_n<T>(st, sc, N);
         gain_p_update<T>(G.c, N, E, Pa, Pa1, Pa2, Pb, Pb1, Pb2);
         for (int q = 0; q < 3; ++q) {
@@ -199,7 +199,7 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
     } else if (which == 1) {
         for (int q = 0; q < 3; ++q) F[q][g] = gain_e_corr<T>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
     } else {
-        double N[4];
+        Pops<T> N;
         T E1[3];
         gain_load_n<T>(st, sc, N);
         for (int q = 0; q < 3; ++q) {

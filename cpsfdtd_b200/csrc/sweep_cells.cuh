@@ -283,7 +283,7 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
     T *st = G.state + c;
     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
-    double N[4];
+    Pops<T> N;
     if (sizeof(T) == 8) {
         using L = GainSite64;
 #pragma unroll
@@ -331,7 +331,7 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
 // gain_warp's.
 struct GainRegs32 {
     float pa[3], pa1[3], pb[3], pb1[3];
-    float n[3];  // N1 - 1, N2, N3
+    float n[3];  // the population offsets N1 - 1, N2, N3
 };
 
 __device__ __forceinline__ uint2 gain_segment(const GainView<float> &G, const Dims &d, int j, int k, int seg,
@@ -372,11 +372,11 @@ __device__ __forceinline__ void gain_apply32(const GainView<float> &G, uint2 m, 
     float Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) { Pa[q] = r.pa[q]; Pa1[q] = r.pa1[q]; Pb[q] = r.pb[q]; Pb1[q] = r.pb1[q]; }
-    double N[4];
-    N[1] = 1.0 + (double)r.n[0];
-    N[2] = (double)r.n[1];
-    N[3] = (double)r.n[2];
-    N[0] = 2.0 - N[1] - N[2] - N[3];  // FP64 conservation, FourLevelLaser.cpp:324
+    Pops<float> N;
+    N.n1 = r.n[0];
+    N.n2 = r.n[1];
+    N.n3 = r.n[2];
+    N.m0 = conserve_m0(N.n1, N.n2, N.n3);  // FP64 conservation, FourLevelLaser.cpp:324
     gain_p_update<float>(G.c, N, E, Pa, Pa1, Pa2, Pb, Pb1, Pb2);
 #pragma unroll
     for (int q = 0; q < 3; ++q) E[q] = gain_e_corr<float>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
