@@ -399,7 +399,7 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
         per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
-            launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, ms);
+            n += launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, ms);
         });
         launch_inject_batch<T>(G, b->d_inj[1], b->ninj[1], 1, s, st);
         for (int c = 0; c < 8; ++c)
@@ -407,7 +407,7 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_dl_batch<T>(G, b->d_dl, b->ndl, st);
         per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
-            launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
+            n += launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
                             FusedShape{b->by, b->kc}, b->d_err, ms);
         });
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
@@ -415,7 +415,6 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, S - 1, st);
         for (int c = 0; c < kNumSweep; ++c) n += b->ntiles[c] > 0;
         n += (b->ndl > 0) + (b->ninj[0] > 0) + (b->ninj[1] > 0) + (b->nsrc > 0) + (b->ngather > 0);
-        for (int gi : b->big) n += 2 + (b->grids[gi]->dl_on && b->grids[gi]->dl_n > 0);
     }
     launch_dft_batch<T>(G, P, b->d_phasor, b->nphasor, b->d_dft, b->ndft, S, st);
     n += b->ndft > 0 ? 2 : 0;

@@ -233,17 +233,15 @@ cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cel
     return upload_raw(g, *d_seg, seg.data(), seg.size() * sizeof(int32_t));
 }
 
-// initial gain state, SoA [word][cell]: all zero (FP32 keeps population
-// offsets) except FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197)
+// initial gain state, groups of 32 cells [group][word][32]: all zero (FP32
+// keeps population offsets) except FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197)
 cps_status gain_state_init(cps_grid *g)
 {
     const int nw = g->fp32 ? kG32Words : kG64Words;
-    CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)g->g_n * nw * g->esz, g->stream));
+    CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)gain_state_elems(g->g_n, nw) * g->esz, g->stream));
     if (!g->fp32 && g->g_n > 0) {
-        const std::vector<double> ones((size_t)g->g_n, 1.0);
-        for (int w : {21, 22})  // FP64 layout words of N0 and N1
-            CK(cudaMemcpyAsync((double *)g->d_g_state + (size_t)w * g->g_n, ones.data(), ones.size() * sizeof(double),
-                               cudaMemcpyHostToDevice, g->stream));
+        launch_gain_init64((double *)g->d_g_state, g->g_n, g->stream);
+        CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(g->stream));
     return CPS_OK;
@@ -643,13 +641,13 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             const bool timed = g->timing_stride > 0 && n % g->timing_stride == 0 &&
                                g->ev_used + 4 <= (int)g->ev.size();
             if (timed) cudaEventRecord(g->ev[g->ev_used], g->stream);
-            if (use_tma) launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
-            else launch_h_fused<T>(f, p, g->shape, g->stream);
+            if (use_tma) g->launches += launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
+            else launch_h_fused<T>(f, p, g->shape, g->stream), g->launches++;
             if (timed) cudaEventRecord(g->ev[g->ev_used + 1], g->stream);
             op_inject<T>(g, 1, (double)n, CPS_FACE_ALL);
             if (timed) cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
-            if (use_tma) launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream);
-            else launch_e_fused<T>(f, p, D, G, g->shape, g->stream);
+            if (use_tma) g->launches += launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream);
+            else launch_e_fused<T>(f, p, D, G, g->shape, g->stream), g->launches++;
             if (g->three_on) {
                 launch_three<T>(f, three_view(g), 3, g->stream);
                 g->launches++;
@@ -660,7 +658,6 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             }
             op_inject<T>(g, 0, (double)n, CPS_FACE_ALL);
             op_sources<T>(g, (int)n);
-            g->launches += 2;
         }
         if (!g->ports.empty()) {
             std::vector<PortState *> all;
@@ -1155,7 +1152,7 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     g->gain_id = p->gain_id;
     if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg, &g->d_g_segm))) return s;
     const int nw = g->fp32 ? kG32Words : kG64Words;
-    if ((s = dalloc(g, &g->d_g_state, (size_t)g->g_n * nw * g->esz))) return s;
+    if ((s = dalloc(g, &g->d_g_state, (size_t)gain_state_elems(g->g_n, nw) * g->esz))) return s;
     if ((s = gain_state_init(g))) return s;
     g->gain_on = true;
     return CPS_OK;
@@ -1717,14 +1714,13 @@ cps_status run_fused_T(cps_grid *g, const std::vector<RecOp> &ops)
     for (const RecOp &o : ops) {
         switch (o.kind) {
         case kOpHBulk:
-            if (use_tma) launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
-            else launch_h_fused<T>(f, p, g->shape, g->stream);
-            g->launches++;
+            if (use_tma) g->launches += launch_h_tma<T>(g->tma, f, p, g->shape, g->d_err, g->stream);
+            else launch_h_fused<T>(f, p, g->shape, g->stream), g->launches++;
             break;
         case kOpEBulk:
-            if (use_tma) launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream);
-            else launch_e_fused<T>(f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->stream);
-            g->launches++;
+            if (use_tma)
+                g->launches += launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream);
+            else launch_e_fused<T>(f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->stream), g->launches++;
             if (g->three_on) {
                 launch_three<T>(f, three_view(g), 3, g->stream);
                 g->launches++;
@@ -2004,7 +2000,7 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
     *ncells = g->g_n;
     if (!out) return CPS_OK;
     const int nw = g->fp32 ? kG32Words : kG64Words;
-    const size_t n = (size_t)g->g_n * nw;
+    const size_t n = (size_t)gain_state_elems(g->g_n, nw);
     std::vector<double> st(n);
     if (g->fp32) {
         std::vector<float> t(n);
@@ -2026,9 +2022,9 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
         ord[c] = {((int64_t)i * (d.ny + 1) + j) * (d.nz + 1) + k, c};
     }
     std::sort(ord.begin(), ord.end());
-    const int64_t sc = g->g_n;
+    const int64_t sc = kGainGroup;
     for (int64_t r = 0; r < g->g_n; ++r) {
-        const int64_t c = ord[r].second;
+        const int64_t c = gain_base_index(ord[r].second, nw);
         double N[4];
         if (g->fp32) {
             N[1] = 1.0 + st[12 * sc + c]; N[2] = st[13 * sc + c]; N[3] = st[14 * sc + c];

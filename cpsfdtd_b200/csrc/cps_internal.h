@@ -83,6 +83,25 @@ struct GainCoef {
 // per-cell gain state words
 constexpr int kG64Words = 25;  // Pa Pa1 Pa2 Pb Pb1 Pb2 (x3 each) E1 (x3) N0..N3
 constexpr int kG32Words = 24;  // Pa Pa1 Pb Pb1 (x3, scaled) dN1 N2 N3 | Pa2 Pb2 E1 (x3, per-routine transients)
+template <typename T>
+__host__ __device__ constexpr int gain_words()
+{
+    return sizeof(T) == 4 ? kG32Words : kG64Words;
+}
+// Gain state storage: the list cells in groups of 32, group q holding word w
+// of its cells at [q][w][32].  Word w of list cell c is then
+// state[gain_base_index(c, words) + w * kGainGroup]: one base per cell and a
+// compile-time offset per word, and a warp's consecutive cells read whole
+// 128-byte lines of every word.
+constexpr int kGainGroup = 32;
+__host__ __device__ inline int64_t gain_base_index(int64_t c, int words)
+{
+    return (c >> 5) * (int64_t)words * kGainGroup + (c & 31);
+}
+__host__ __device__ inline int64_t gain_state_elems(int64_t ncell, int words)
+{
+    return ((ncell + kGainGroup - 1) / kGainGroup) * (int64_t)words * kGainGroup;
+}
 
 // --- TF/SF / source injection in CSR form: each target (cell, component)
 // owns a run of contributions applied in the reference's face order.
@@ -215,6 +234,8 @@ template <typename T> void launch_h_pml(const FieldView<T> &f, const PmlView<T> 
 template <typename T> void launch_e_pml(const FieldView<T> &f, const PmlView<T> &p, cudaStream_t s);
 template <typename T> void launch_dl(const FieldView<T> &f, const DlView<T> &d, cudaStream_t s);
 template <typename T> void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStream_t s);
+// initial gain state: FP64 N0 = N1 = 1 in every group (the rest zeroed by the caller)
+void launch_gain_init64(double *state, int64_t ncell, cudaStream_t s);
 // three-level gain sites: which 0 polarisation, 1 E field, 2 populations, 3 all
 // three in order (kernels_three.cu, no FMA contraction); init: zero state, N0 = N_0
 template <typename T> void launch_three(const FieldView<T> &f, const ThreeView &t, int which, cudaStream_t s);
@@ -242,12 +263,14 @@ void launch_e_fused(const FieldView<T> &f, const PmlView<T> &p, const DlView<T> 
 }  // namespace cps
 #include "tma.cuh"
 namespace cps {
+// (each sweep launches its CPML tiles and its interior tiles separately;
+// the return value is the number of kernels launched)
 template <typename T>
-void launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
-                  cudaStream_t s);
+int launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
+                 cudaStream_t s);
 template <typename T>
-void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                  const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s);
+int launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s);
 // set the shared-memory attributes of every TMA sweep kernel (call outside captures)
 template <typename T>
 void tma_attributes();

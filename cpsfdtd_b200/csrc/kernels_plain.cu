@@ -178,8 +178,8 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
 {
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= G.ncell) return;
-    const int64_t g = G.cell[c], sc = G.ncell;
-    T *st = G.state + c;
+    const int64_t g = G.cell[c], sc = kGainGroup;
+    T *st = G.state + gain_base_index(c, gain_words<T>());
     T *F[3] = {f.Ex, f.Ey, f.Ez};
     T E[3] = {F[0][g], F[1][g], F[2][g]};
     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
@@ -208,6 +208,16 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
         gain_n_update<T>(G.c, N, E, E1, Pa, Pa1, Pa2, Pb, Pb2);
         gain_store_n<T>(st, sc, N);
     }
+}
+
+// FP64 initial populations N0 = N1 = 1 (words 21, 22 of each cell)
+__global__ void k_gain_init64(double *state, int64_t ncell)
+{
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    double *st = state + gain_base_index(c, kG64Words);
+    st[GainSite64::N * kGainGroup] = 1.0;
+    st[(GainSite64::N + 1) * kGainGroup] = 1.0;
 }
 
 // TF/SF (and any other table-driven) injection in CSR form: each thread owns
@@ -375,6 +385,12 @@ void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStr
         k_gain<T, GainSite64><<<cdiv(g.ncell, 128), 128, 0, s>>>(f, g, which);
     else
         k_gain<T, GainSite32><<<cdiv(g.ncell, 128), 128, 0, s>>>(f, g, which);
+}
+
+void launch_gain_init64(double *state, int64_t ncell, cudaStream_t s)
+{
+    if (ncell <= 0) return;
+    k_gain_init64<<<cdiv(ncell, 256), 256, 0, s>>>(state, ncell);
 }
 
 template <typename T>

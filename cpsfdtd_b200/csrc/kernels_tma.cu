@@ -1,6 +1,9 @@
 // kernels_tma.cu -- one-grid launches of the TMA-fed fused H and E sweeps
 // (sm_100a): one block per 32 x BY x kc tile, bodies in tma_bodies.cuh.
 #include <cuda.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "tma_bodies.cuh"
 
@@ -8,40 +11,37 @@ namespace cps {
 
 namespace {
 
+// One block per tile of the launch's boxes; PML: every tile of this launch
+// meets a CPML slab (the CPML body), otherwise none does.
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
-__global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 * BY)) k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
-                                                    DlView<T> D, GainView<T> G, int kc, int *err)
+__global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 * BY))
+    k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc,
+            const __grid_constant__ TileBoxes tb, int *err)
 {
     extern __shared__ __align__(128) unsigned char sm_raw[];
     __shared__ __align__(8) uint64_t full[kStages];
     unsigned char *sm = align_smem(sm_raw);
-    const TileXYZ t{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z};
+    const TileXYZ t = box_tile(tb, (int)blockIdx.x);
     const int k0 = max(1, t.bz * kc), k1 = min(t.bz * kc + kc, f.d.nz);
     if (k0 >= k1) return;
     init_stages(full);
     uint32_t ctr = 0;
-    if (PML && tile_in_pml(p.np, f.d, t.bx * 32, t.by * BY, BY, k0, k1, true))
-        e_tma_body<T, BY, true, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
-    else
-        e_tma_body<T, BY, false, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
+    e_tma_body<T, BY, PML, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
 }
 
 template <typename T, int BY, bool PML>
 __global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
-                                                    int kc, int *err)
+                                                    int kc, const __grid_constant__ TileBoxes tb, int *err)
 {
     extern __shared__ __align__(128) unsigned char sm_raw[];
     __shared__ __align__(8) uint64_t full[kStages];
     unsigned char *sm = align_smem(sm_raw);
-    const TileXYZ t{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z};
+    const TileXYZ t = box_tile(tb, (int)blockIdx.x);
     const int k0 = t.bz * kc, k1 = min(k0 + kc, f.d.nz);
     if (k0 >= k1) return;
     init_stages(full);
     uint32_t ctr = 0;
-    if (PML && tile_in_pml(p.np, f.d, t.bx * 32, t.by * BY, BY, k0, k1, false))
-        h_tma_body<T, BY, true>(M, f, p, kc, t, ctr, err, sm, full);
-    else
-        h_tma_body<T, BY, false>(M, f, p, kc, t, ctr, err, sm, full);
+    h_tma_body<T, BY, PML>(M, f, p, kc, t, ctr, err, sm, full);
 }
 
 // The ID-2 cells the TMA E sweep leaves alone, one thread per cell of the
@@ -64,23 +64,88 @@ bool set_smem(int bytes)
     return kernel_smem<K>(bytes);
 }
 
+// Interior and CPML tiles of a sweep as tile boxes.  A tile meets a CPML slab
+// when its x, y or z range does (tile_in_pml in tma_bodies.cuh, per axis), so
+// the interior tiles form one box [a0, a1) per axis and the CPML tiles the
+// rest: below and above the interior in z (whole planes of tiles), then in y,
+// then in x.
+struct SweepTiles {
+    TileBoxes interior, pml;
+};
+
+inline void add_box(TileBoxes &b, int x0, int x1, int y0, int y1, int z0, int z1)
+{
+    if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
+    const int k = b.n++;
+    b.bx0[k] = x0; b.by0[k] = y0; b.bz0[k] = z0;
+    b.nbx[k] = x1 - x0; b.nby[k] = y1 - y0;
+    b.start[k + 1] = b.start[k] + (x1 - x0) * (y1 - y0) * (z1 - z0);
+}
+
+inline SweepTiles sweep_tiles(const int np[6], bool pml_on, const Dims &d, int by, int kc, bool eside)
+{
+    const int tx = (int)cdiv(d.nx, 32), ty = (int)cdiv(d.ny, by), tz = (int)cdiv(d.nz, kc);
+    SweepTiles t;
+    memset(&t, 0, sizeof(t));
+    if (!pml_on) {
+        add_box(t.interior, 0, tx, 0, ty, 0, tz);
+        return t;
+    }
+    const int lo = eside ? 0 : 1;
+    // per axis: the first and one-past-last tile index that meets no slab
+    auto interval = [](int n, auto in_slab, int &a0, int &a1) {
+        a0 = 0;
+        while (a0 < n && in_slab(a0)) ++a0;
+        a1 = a0;
+        while (a1 < n && !in_slab(a1)) ++a1;
+        for (int q = a1; q < n; ++q)
+            if (!in_slab(q)) { a0 = a1 = 0; return; }  // not one interval: every tile takes the CPML body
+    };
+    int ax0, ax1, ay0, ay1, az0, az1;
+    interval(tx, [&](int b) { const int x0 = 32 * b; return x0 <= np[kFX1] - lo || x0 + 31 >= d.nx - np[kFX2]; },
+             ax0, ax1);
+    interval(ty, [&](int b) { const int y0 = by * b; return y0 <= np[kFY1] - lo || y0 + by - 1 >= d.ny - np[kFY2]; },
+             ay0, ay1);
+    interval(tz, [&](int b) {
+        const int k0 = eside ? std::max(1, b * kc) : b * kc, k1 = std::min(b * kc + kc, d.nz);
+        return k0 <= np[kFZ1] - lo || k1 - 1 >= d.nz - np[kFZ2];
+    }, az0, az1);
+    if (ax1 <= ax0 || ay1 <= ay0 || az1 <= az0) {
+        add_box(t.pml, 0, tx, 0, ty, 0, tz);
+        return t;
+    }
+    add_box(t.interior, ax0, ax1, ay0, ay1, az0, az1);
+    add_box(t.pml, 0, tx, 0, ty, 0, az0);
+    add_box(t.pml, 0, tx, 0, ty, az1, tz);
+    add_box(t.pml, 0, tx, 0, ay0, az0, az1);
+    add_box(t.pml, 0, tx, ay1, ty, az0, az1);
+    add_box(t.pml, 0, ax0, ay0, ay1, az0, az1);
+    add_box(t.pml, ax1, tx, ay0, ay1, az0, az1);
+    return t;
+}
+
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
-void e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                  const GainView<T> &G, int kc, int *err, cudaStream_t s)
+int e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+                 const GainView<T> &G, int kc, const TileBoxes &tb, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    if (!set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM)) return;
-    dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
-    k_e_tma<T, BY, PML, DL, GAIN><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, err);
+    const int blocks = tb.start[tb.n];
+    if (blocks <= 0) return 0;
+    if (!set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM)) return 0;
+    k_e_tma<T, BY, PML, DL, GAIN><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, tb, err);
+    return 1;
 }
 
 template <typename T, int BY, bool PML>
-void h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, int *err, cudaStream_t s)
+int h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, const TileBoxes &tb,
+                 int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
-    if (!set_smem<k_h_tma<T, BY, PML>>(L::SMEM)) return;
-    dim3 grid(cdiv(f.d.nx, 32), cdiv(f.d.ny, BY), cdiv(f.d.nz, kc));
-    k_h_tma<T, BY, PML><<<grid, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, err);
+    const int blocks = tb.start[tb.n];
+    if (blocks <= 0) return 0;
+    if (!set_smem<k_h_tma<T, BY, PML>>(L::SMEM)) return 0;
+    k_h_tma<T, BY, PML><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, tb, err);
+    return 1;
 }
 
 template <typename T, int BY>
@@ -99,49 +164,54 @@ void attrs_by()
     set_smem<k_e_tma<T, BY, true, true, true>>(S);
 }
 
-template <typename T, int BY>
-void e_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-              const GainView<T> &G, int kc, int *err, cudaStream_t s)
+template <typename T, int BY, bool PML>
+int e_tma_class(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+                const GainView<T> &G, int kc, const TileBoxes &tb, int *err, cudaStream_t s)
 {
     const bool dl = D.on && D.ncell > 0, gn = G.on && G.ncell > 0;
-    if (p.on) {
-        if (dl && gn) e_tma_launch<T, BY, true, true, true>(M, f, p, D, G, kc, err, s);
-        else if (dl) e_tma_launch<T, BY, true, true, false>(M, f, p, D, G, kc, err, s);
-        else if (gn) e_tma_launch<T, BY, true, false, true>(M, f, p, D, G, kc, err, s);
-        else e_tma_launch<T, BY, true, false, false>(M, f, p, D, G, kc, err, s);
-    } else {
-        if (dl && gn) e_tma_launch<T, BY, false, true, true>(M, f, p, D, G, kc, err, s);
-        else if (dl) e_tma_launch<T, BY, false, true, false>(M, f, p, D, G, kc, err, s);
-        else if (gn) e_tma_launch<T, BY, false, false, true>(M, f, p, D, G, kc, err, s);
-        else e_tma_launch<T, BY, false, false, false>(M, f, p, D, G, kc, err, s);
-    }
+    if (dl && gn) return e_tma_launch<T, BY, PML, true, true>(M, f, p, D, G, kc, tb, err, s);
+    if (dl) return e_tma_launch<T, BY, PML, true, false>(M, f, p, D, G, kc, tb, err, s);
+    if (gn) return e_tma_launch<T, BY, PML, false, true>(M, f, p, D, G, kc, tb, err, s);
+    return e_tma_launch<T, BY, PML, false, false>(M, f, p, D, G, kc, tb, err, s);
+}
+
+template <typename T, int BY>
+int e_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+             const GainView<T> &G, int kc, int *err, cudaStream_t s)
+{
+    const SweepTiles t = sweep_tiles(p.np, p.on, f.d, BY, kc, true);
+    return e_tma_class<T, BY, true>(M, f, p, D, G, kc, t.pml, err, s) +
+           e_tma_class<T, BY, false>(M, f, p, D, G, kc, t.interior, err, s);
+}
+
+template <typename T, int BY>
+int h_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, int *err, cudaStream_t s)
+{
+    const SweepTiles t = sweep_tiles(p.np, p.on, f.d, BY, kc, false);
+    return h_tma_launch<T, BY, true>(M, f, p, kc, t.pml, err, s) +
+           h_tma_launch<T, BY, false>(M, f, p, kc, t.interior, err, s);
 }
 
 }  // namespace
 
 template <typename T>
-void launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
-                  cudaStream_t s)
+int launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
+                 cudaStream_t s)
 {
-    if (sh.by == 4) {
-        if (p.on) h_tma_launch<T, 4, true>(M, f, p, sh.kc, err, s);
-        else h_tma_launch<T, 4, false>(M, f, p, sh.kc, err, s);
-    } else {
-        if (p.on) h_tma_launch<T, 8, true>(M, f, p, sh.kc, err, s);
-        else h_tma_launch<T, 8, false>(M, f, p, sh.kc, err, s);
-    }
+    return sh.by == 4 ? h_tma_by<T, 4>(M, f, p, sh.kc, err, s) : h_tma_by<T, 8>(M, f, p, sh.kc, err, s);
 }
 
 template <typename T>
-void launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                  const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s)
+int launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
+                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s)
 {
-    if (sh.by == 4) e_tma_by<T, 4>(M, f, p, D, G, sh.kc, err, s);
-    else e_tma_by<T, 8>(M, f, p, D, G, sh.kc, err, s);
+    int n = sh.by == 4 ? e_tma_by<T, 4>(M, f, p, D, G, sh.kc, err, s) : e_tma_by<T, 8>(M, f, p, D, G, sh.kc, err, s);
     if (D.on && D.ncell > 0) {
         if (p.on) k_dl_cells<T, true><<<cdiv(D.ncell, 128), 128, 0, s>>>(f, p, D);
         else k_dl_cells<T, false><<<cdiv(D.ncell, 128), 128, 0, s>>>(f, p, D);
+        ++n;
     }
+    return n;
 }
 
 template <typename T>
@@ -153,13 +223,13 @@ void tma_attributes()
 
 template void tma_attributes<float>();
 template void tma_attributes<double>();
-template void launch_h_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &, FusedShape, int *,
+template int launch_h_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &, FusedShape, int *,
                                   cudaStream_t);
-template void launch_h_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &, FusedShape,
+template int launch_h_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &, FusedShape,
                                    int *, cudaStream_t);
-template void launch_e_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &,
+template int launch_e_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &,
                                   const DlView<float> &, const GainView<float> &, FusedShape, int *, cudaStream_t);
-template void launch_e_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &,
+template int launch_e_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &,
                                    const DlView<double> &, const GainView<double> &, FusedShape, int *, cudaStream_t);
 
 }  // namespace cps

@@ -279,8 +279,8 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
     const int nseg = d.px >> 5;
     const int64_t base = G.seg[((int64_t)k * (d.ny + 1) + j) * nseg + seg];
     if (!mine) return;
-    const int64_t c = base + __popc(m & lanemask_lt()), sc = G.ncell;
-    T *st = G.state + c;
+    const int64_t c = base + __popc(m & lanemask_lt()), sc = kGainGroup;
+    T *st = G.state + gain_base_index(c, gain_words<T>());
     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
     Pops<T> N;
@@ -345,8 +345,8 @@ __device__ __forceinline__ void gain_fetch32(const GainView<float> &G, uint2 m, 
     const unsigned lane = threadIdx.x & 31u;
     if (!((m.y >> lane) & 1u)) return;
     using L = GainSite32;
-    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = G.ncell;
-    const float *st = G.state + c;
+    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = kGainGroup;
+    const float *st = G.state + gain_base_index(c, kG32Words);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
         r.pa[q] = __ldg(st + (L::PA + q) * sc);
@@ -366,8 +366,8 @@ __device__ __forceinline__ void gain_apply32(const GainView<float> &G, uint2 m, 
     const unsigned lane = threadIdx.x & 31u;
     if (!((m.y >> lane) & 1u)) return;
     using L = GainSite32;
-    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = G.ncell;
-    float *st = G.state + c;
+    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = kGainGroup;
+    float *st = G.state + gain_base_index(c, kG32Words);
     float E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
     float Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
 #pragma unroll

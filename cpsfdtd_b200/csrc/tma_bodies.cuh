@@ -121,6 +121,28 @@ __device__ __forceinline__ bool tile_in_pml(const int np[6], const Dims &d, int 
     return x || y || z;
 }
 
+// Up to six boxes of tiles (in tile coordinates) covered by one launch, one
+// block per tile: a sweep launches its interior tiles (one box, the CPML-free
+// body) and its CPML tiles (the rest of the grid, up to six boxes) separately,
+// so the interior blocks are not held to the CPML body's register count.
+struct TileBoxes {
+    int n;         // boxes in use
+    int start[7];  // first block of each box; start[n] = blocks in the launch
+    int bx0[6], by0[6], bz0[6];
+    int nbx[6], nby[6];
+};
+
+__device__ __forceinline__ TileXYZ box_tile(const TileBoxes &b, int q)
+{
+    int k = 0;
+    while (k + 1 < b.n && q >= b.start[k + 1]) ++k;
+    const int r = q - b.start[k];
+    const int nxy = b.nbx[k] * b.nby[k];
+    const int z = r / nxy, rem = r - z * nxy;
+    const int y = rem / b.nbx[k];
+    return TileXYZ{b.bx0[k] + rem - y * b.nbx[k], b.by0[k] + y, b.bz0[k] + z};
+}
+
 // E sweep of one tile: planes max(1, bz*kc) .. min(bz*kc+kc, nz)-1.
 template <typename T, int BY, bool PML, bool DL, bool GAIN>
 __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p,
