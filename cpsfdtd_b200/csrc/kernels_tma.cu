@@ -11,9 +11,13 @@ namespace cps {
 
 namespace {
 
-// One block per tile of the launch's boxes; PML: every tile of this launch
-// meets a CPML slab (the CPML body), otherwise none does.
-template <typename T, int BY, bool PML, bool DL, bool GAIN>
+// One block per tile of the launch's boxes.  PM selects the body: 0 the
+// CPML-free body for every tile, 1 the CPML body for every tile, 2 the body
+// each tile needs (tile_in_pml).  A sweep with gain launches its CPML tiles
+// (PM 1) and interior tiles (PM 0) separately, so the interior blocks are not
+// held to the CPML body's register count; other sweeps run one launch (PM 2),
+// where a second launch's extra partial wave would cost more than it saves.
+template <typename T, int BY, int PM, bool DL, bool GAIN>
 __global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 * BY))
     k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc,
             const __grid_constant__ TileBoxes tb, int *err)
@@ -26,10 +30,13 @@ __global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 *
     if (k0 >= k1) return;
     init_stages(full);
     uint32_t ctr = 0;
-    e_tma_body<T, BY, PML, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
+    if (PM == 1 || (PM == 2 && tile_in_pml(p.np, f.d, t.bx * 32, t.by * BY, BY, k0, k1, true)))
+        e_tma_body<T, BY, PM != 0, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
+    else
+        e_tma_body<T, BY, false, DL, GAIN>(M, f, p, D, G, kc, t, ctr, err, sm, full);
 }
 
-template <typename T, int BY, bool PML>
+template <typename T, int BY, int PM>
 __global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p,
                                                     int kc, const __grid_constant__ TileBoxes tb, int *err)
 {
@@ -41,7 +48,10 @@ __global__ void __launch_bounds__(32 * BY) k_h_tma(const __grid_constant__ TmaMa
     if (k0 >= k1) return;
     init_stages(full);
     uint32_t ctr = 0;
-    h_tma_body<T, BY, PML>(M, f, p, kc, t, ctr, err, sm, full);
+    if (PM == 1 || (PM == 2 && tile_in_pml(p.np, f.d, t.bx * 32, t.by * BY, BY, k0, k1, false)))
+        h_tma_body<T, BY, PM != 0>(M, f, p, kc, t, ctr, err, sm, full);
+    else
+        h_tma_body<T, BY, false>(M, f, p, kc, t, ctr, err, sm, full);
 }
 
 // The ID-2 cells the TMA E sweep leaves alone, one thread per cell of the
@@ -80,6 +90,15 @@ inline void add_box(TileBoxes &b, int x0, int x1, int y0, int y1, int z0, int z1
     b.bx0[k] = x0; b.by0[k] = y0; b.bz0[k] = z0;
     b.nbx[k] = x1 - x0; b.nby[k] = y1 - y0;
     b.start[k + 1] = b.start[k] + (x1 - x0) * (y1 - y0) * (z1 - z0);
+}
+
+// every tile of the grid as one box
+inline TileBoxes whole_grid(const Dims &d, int by, int kc)
+{
+    TileBoxes b;
+    memset(&b, 0, sizeof(b));
+    add_box(b, 0, (int)cdiv(d.nx, 32), 0, (int)cdiv(d.ny, by), 0, (int)cdiv(d.nz, kc));
+    return b;
 }
 
 inline SweepTiles sweep_tiles(const int np[6], bool pml_on, const Dims &d, int by, int kc, bool eside)
@@ -124,72 +143,73 @@ inline SweepTiles sweep_tiles(const int np[6], bool pml_on, const Dims &d, int b
     return t;
 }
 
-template <typename T, int BY, bool PML, bool DL, bool GAIN>
+template <typename T, int BY, int PM, bool DL, bool GAIN>
 int e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
                  const GainView<T> &G, int kc, const TileBoxes &tb, int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
     const int blocks = tb.start[tb.n];
     if (blocks <= 0) return 0;
-    if (!set_smem<k_e_tma<T, BY, PML, DL, GAIN>>(L::SMEM)) return 0;
-    k_e_tma<T, BY, PML, DL, GAIN><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, tb, err);
+    if (!set_smem<k_e_tma<T, BY, PM, DL, GAIN>>(L::SMEM)) return 0;
+    k_e_tma<T, BY, PM, DL, GAIN><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, D, G, kc, tb, err);
     return 1;
 }
 
-template <typename T, int BY, bool PML>
+template <typename T, int BY, int PM>
 int h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, const TileBoxes &tb,
                  int *err, cudaStream_t s)
 {
     using L = StageLayout<T, BY>;
     const int blocks = tb.start[tb.n];
     if (blocks <= 0) return 0;
-    if (!set_smem<k_h_tma<T, BY, PML>>(L::SMEM)) return 0;
-    k_h_tma<T, BY, PML><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, tb, err);
+    if (!set_smem<k_h_tma<T, BY, PM>>(L::SMEM)) return 0;
+    k_h_tma<T, BY, PM><<<blocks, dim3(32, BY), L::SMEM, s>>>(M, f, p, kc, tb, err);
     return 1;
 }
 
+// the kernels the launchers below use (CPML-free, per-tile, and for gain the
+// two halves of the split)
 template <typename T, int BY>
 void attrs_by()
 {
     constexpr int S = StageLayout<T, BY>::SMEM;
-    set_smem<k_h_tma<T, BY, false>>(S);
-    set_smem<k_h_tma<T, BY, true>>(S);
-    set_smem<k_e_tma<T, BY, false, false, false>>(S);
-    set_smem<k_e_tma<T, BY, false, false, true>>(S);
-    set_smem<k_e_tma<T, BY, false, true, false>>(S);
-    set_smem<k_e_tma<T, BY, false, true, true>>(S);
-    set_smem<k_e_tma<T, BY, true, false, false>>(S);
-    set_smem<k_e_tma<T, BY, true, false, true>>(S);
-    set_smem<k_e_tma<T, BY, true, true, false>>(S);
-    set_smem<k_e_tma<T, BY, true, true, true>>(S);
-}
-
-template <typename T, int BY, bool PML>
-int e_tma_class(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                const GainView<T> &G, int kc, const TileBoxes &tb, int *err, cudaStream_t s)
-{
-    const bool dl = D.on && D.ncell > 0, gn = G.on && G.ncell > 0;
-    if (dl && gn) return e_tma_launch<T, BY, PML, true, true>(M, f, p, D, G, kc, tb, err, s);
-    if (dl) return e_tma_launch<T, BY, PML, true, false>(M, f, p, D, G, kc, tb, err, s);
-    if (gn) return e_tma_launch<T, BY, PML, false, true>(M, f, p, D, G, kc, tb, err, s);
-    return e_tma_launch<T, BY, PML, false, false>(M, f, p, D, G, kc, tb, err, s);
+    set_smem<k_h_tma<T, BY, 0>>(S);
+    set_smem<k_h_tma<T, BY, 2>>(S);
+    set_smem<k_e_tma<T, BY, 0, false, false>>(S);
+    set_smem<k_e_tma<T, BY, 0, false, true>>(S);
+    set_smem<k_e_tma<T, BY, 0, true, false>>(S);
+    set_smem<k_e_tma<T, BY, 0, true, true>>(S);
+    set_smem<k_e_tma<T, BY, 2, false, false>>(S);
+    set_smem<k_e_tma<T, BY, 2, true, false>>(S);
+    set_smem<k_e_tma<T, BY, 1, false, true>>(S);
+    set_smem<k_e_tma<T, BY, 1, true, true>>(S);
 }
 
 template <typename T, int BY>
 int e_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
              const GainView<T> &G, int kc, int *err, cudaStream_t s)
 {
+    const bool dl = D.on && D.ncell > 0, gn = G.on && G.ncell > 0;
     const SweepTiles t = sweep_tiles(p.np, p.on, f.d, BY, kc, true);
-    return e_tma_class<T, BY, true>(M, f, p, D, G, kc, t.pml, err, s) +
-           e_tma_class<T, BY, false>(M, f, p, D, G, kc, t.interior, err, s);
+    if (gn) {  // CPML tiles (if any) and interior tiles as two launches
+        return (dl ? e_tma_launch<T, BY, 1, true, true>(M, f, p, D, G, kc, t.pml, err, s)
+                   : e_tma_launch<T, BY, 1, false, true>(M, f, p, D, G, kc, t.pml, err, s)) +
+               (dl ? e_tma_launch<T, BY, 0, true, true>(M, f, p, D, G, kc, t.interior, err, s)
+                   : e_tma_launch<T, BY, 0, false, true>(M, f, p, D, G, kc, t.interior, err, s));
+    }
+    const TileBoxes all = whole_grid(f.d, BY, kc);
+    if (p.on)
+        return dl ? e_tma_launch<T, BY, 2, true, false>(M, f, p, D, G, kc, all, err, s)
+                  : e_tma_launch<T, BY, 2, false, false>(M, f, p, D, G, kc, all, err, s);
+    return dl ? e_tma_launch<T, BY, 0, true, false>(M, f, p, D, G, kc, all, err, s)
+              : e_tma_launch<T, BY, 0, false, false>(M, f, p, D, G, kc, all, err, s);
 }
 
 template <typename T, int BY>
 int h_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, int kc, int *err, cudaStream_t s)
 {
-    const SweepTiles t = sweep_tiles(p.np, p.on, f.d, BY, kc, false);
-    return h_tma_launch<T, BY, true>(M, f, p, kc, t.pml, err, s) +
-           h_tma_launch<T, BY, false>(M, f, p, kc, t.interior, err, s);
+    const TileBoxes all = whole_grid(f.d, BY, kc);
+    return p.on ? h_tma_launch<T, BY, 2>(M, f, p, kc, all, err, s) : h_tma_launch<T, BY, 0>(M, f, p, kc, all, err, s);
 }
 
 }  // namespace
