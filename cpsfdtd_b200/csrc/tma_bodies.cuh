@@ -307,48 +307,53 @@ __device__ __forceinline__ bool h_tma_body(const TmaMaps &M, const FieldView<T> 
         }
     }
     T ex = ((const T *)(sm + s0 * L::STAGE_B))[er], ey = ((const T *)(sm + s0 * L::STAGE_B + L::HALO_B))[er];
-    PsiRegs<T> qc{}, qn{}, qnn{};
-    if (PML && act) {
-        psi_load_h(p, d, pc, i, j, k0, qc);
-        if (k0 + 1 < k1) psi_load_h(p, d, pc, i, j, k0 + 1, qn);
-    }
-    for (int k = k0, it = 0; k < k1; ++k, ++it) {
-        if (PML && act && k + 2 < k1) psi_load_h(p, d, pc, i, j, k + 2, qnn);  // psi two planes ahead
-        const uint32_t q = c0 + (uint32_t)it, qn1 = q + 1u;
-        const int s = (int)(q % kStages), sn = (int)(qn1 % kStages);
-        const bool ok = wait_stage(&full[sn], (qn1 / kStages) & 1u);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                atomicExch(err, 2);
-                drain_stages(full, c0, it + 2, min(it + kStages - 1, npl));
+    // psi of plane k+1 requested at the top of plane k into the other of two
+    // register slots (the loop is unrolled by two, so the slots are never copied)
+    PsiRegs<T> qA{}, qB{};
+    if (PML && act) psi_load_h(p, d, pc, i, j, k0, qA);
+    for (int kb = k0, itb = 0; kb < k1; kb += 2, itb += 2) {
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int k = kb + u, it = itb + u;
+            if (k >= k1) break;
+            PsiRegs<T> &qc = u == 0 ? qA : qB, &qn = u == 0 ? qB : qA;
+            if (PML && act && k + 1 < k1) psi_load_h(p, d, pc, i, j, k + 1, qn);
+            const uint32_t q = c0 + (uint32_t)it, qn1 = q + 1u;
+            const int s = (int)(q % kStages), sn = (int)(qn1 % kStages);
+            const bool ok = wait_stage(&full[sn], (qn1 / kStages) & 1u);
+            if (__syncthreads_or(!ok)) {
+                if (tid == 0) {
+                    atomicExch(err, 2);
+                    drain_stages(full, c0, it + 2, min(it + kStages - 1, npl));
+                }
+                return false;
             }
-            return false;
+            const unsigned char *b = sm + s * L::STAGE_B, *bn = sm + sn * L::STAGE_B;
+            const T *ext = (const T *)b, *eyt = (const T *)(b + L::HALO_B), *ezt = (const T *)(b + 2 * L::HALO_B);
+            const T *hxt = (const T *)(b + 3 * L::HALO_B), *hyt = (const T *)(b + 3 * L::HALO_B + L::OWN_B);
+            const T *hzt = (const T *)(b + 3 * L::HALO_B + 2 * L::OWN_B);
+            const uint8_t *idt = b + 3 * L::HALO_B + 3 * L::OWN_B;
+            const T exk = ((const T *)bn)[er], eyk = ((const T *)(bn + L::HALO_B))[er];
+            const T ez = ezt[er];
+            const T dEz_i = ezt[er + 1] - ez, dEz_j = ezt[er + L::HW] - ez;
+            const T dEx_j = ext[er + L::HW] - ex, dEy_i = eyt[er + 1] - ey;
+            const T dEx_k = exk - ex, dEy_k = eyk - ey;
+            const int id = idt[orow];
+            const T aH = __ldg(&f.aH[id]), bH = __ldg(&f.bH[id]);
+            T hx = aH * hxt[orow] - bH * dEz_j * cHxz + bH * dEy_k * sv.cHxy[k];
+            T hy = aH * hyt[orow] - bH * dEx_k * sv.cHyx[k] + bH * dEz_i * cHyz;
+            T hz = aH * hzt[orow] + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
+            if (act) {
+                if (PML)
+                    pml_h_cell_pre(p, d, pc, pml_ch_cell(p, f.bH, id), i, j, k, qc, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k,
+                                   dEx_k, hx, hy, hz);
+                const int64_t g = d.idx(i, j, k);
+                f.Hx[g] = hx; f.Hy[g] = hy; f.Hz[g] = hz;
+            }
+            ex = exk; ey = eyk;
+            __syncthreads();
+            if (tid == 0 && k + kStages <= k1) issue(it + kStages, k + kStages);
         }
-        const unsigned char *b = sm + s * L::STAGE_B, *bn = sm + sn * L::STAGE_B;
-        const T *ext = (const T *)b, *eyt = (const T *)(b + L::HALO_B), *ezt = (const T *)(b + 2 * L::HALO_B);
-        const T *hxt = (const T *)(b + 3 * L::HALO_B), *hyt = (const T *)(b + 3 * L::HALO_B + L::OWN_B);
-        const T *hzt = (const T *)(b + 3 * L::HALO_B + 2 * L::OWN_B);
-        const uint8_t *idt = b + 3 * L::HALO_B + 3 * L::OWN_B;
-        const T exk = ((const T *)bn)[er], eyk = ((const T *)(bn + L::HALO_B))[er];
-        const T ez = ezt[er];
-        const T dEz_i = ezt[er + 1] - ez, dEz_j = ezt[er + L::HW] - ez;
-        const T dEx_j = ext[er + L::HW] - ex, dEy_i = eyt[er + 1] - ey;
-        const T dEx_k = exk - ex, dEy_k = eyk - ey;
-        const int id = idt[orow];
-        const T aH = __ldg(&f.aH[id]), bH = __ldg(&f.bH[id]);
-        T hx = aH * hxt[orow] - bH * dEz_j * cHxz + bH * dEy_k * sv.cHxy[k];
-        T hy = aH * hyt[orow] - bH * dEx_k * sv.cHyx[k] + bH * dEz_i * cHyz;
-        T hz = aH * hzt[orow] + bH * dEx_j * cHzx - bH * dEy_i * cHzy;
-        if (act) {
-            if (PML) pml_h_cell_pre(p, d, pc, pml_ch_cell(p, f.bH, id), i, j, k, qc, dEz_i, dEy_i, dEx_j, dEz_j, dEy_k, dEx_k, hx, hy, hz);
-            const int64_t g = d.idx(i, j, k);
-            f.Hx[g] = hx; f.Hy[g] = hy; f.Hz[g] = hz;
-        }
-        ex = exk; ey = eyk;
-        qc = qn;
-        qn = qnn;
-        __syncthreads();
-        if (tid == 0 && k + kStages <= k1) issue(it + kStages, k + kStages);
     }
     ctr = c0 + (uint32_t)(k1 - k0 + 1);
     return true;
