@@ -489,6 +489,31 @@ def fp64_legs(prep, args, local, dist):
     return out
 
 
+def fp64_with_peak(dk, steps, local, checkpoints=20):
+    """The deck alone in FP64 on the fused path, stepped in chunks; returns the
+    grid and, per field component, the largest L2 norm seen at the
+    checkpoints (the scale against which a decayed final field's error is
+    read)."""
+    import cpsfdtd_b200 as cps
+    g = cps.Grid.from_deck(dk, cps.FP64, device=local)
+    peak = np.zeros(6)
+    chunk = max(1, -(-steps // checkpoints))
+    done = 0
+    while done < steps:
+        n = min(chunk, steps - done)
+        g.step(n, cps.FUSED)
+        done += n
+        peak = np.maximum(peak, [float(np.linalg.norm(g.field(c))) for c in range(6)])
+    g.sync()
+    return g, peak
+
+
+def err_vs_peak(a_fields, b_fields, peak):
+    """max over components of |a - b|_2 / (the component's peak norm)"""
+    return max(float(np.linalg.norm(np.asarray(x, np.float64) - np.asarray(y, np.float64))) / p
+               for x, y, p in zip(a_fields, b_fields, peak) if p > 0)
+
+
 def grid_report(a, b, dk):
     """accuracy of grid a against grid b: fields and every DFT port"""
     from cpsfdtd_b200 import accuracy
@@ -549,10 +574,9 @@ def accuracy_legs(args, local, c3_prep, c2_prep):
         b.add(g)
     b.step(5000)
     b.sync()
-    ref = cps.Grid.from_deck(dks[0], cps.FP64, device=local)
-    ref.step(5000, cps.FUSED)
-    ref.sync()
+    ref, peak = fp64_with_peak(dks[0], 5000, local)
     r = grid_report(gs[0], ref, dks[0])
+    r["field_err_vs_peak"] = err_vs_peak([gs[0].field(c) for c in range(6)], [ref.field(c) for c in range(6)], peak)
     r.update({"time_steps": 5000, "grid": [128, 128, 128], "form": "fp32 batched (3 members) vs fp64 alone"})
     rep["c4"] = r
     b.close()
@@ -755,9 +779,7 @@ def serving(args, local):
             continue
         _, edge, steps, seed = jobs[n]
         dk = serve_deck(kind, edge, steps, seed)
-        g = cps.Grid.from_deck(dk, cps.FP64, device=local)
-        g.step(steps, cps.FUSED)
-        g.sync()
+        g, peak = fp64_with_peak(dk, steps, local)
         fields, dfts = kept[n]
         ports = []
         k = 0
@@ -765,7 +787,10 @@ def serving(args, local):
             if p.dft_freqs is not None:
                 ports.append(accuracy.port_errors(p.dft_freqs, dfts[k], g.port_dft(p_i, raw=True)))
                 k += 1
-        r = accuracy.summarize(accuracy.field_errors(fields, [g.field(c) for c in range(6)]), ports)
+        ref = [g.field(c) for c in range(6)]
+        r = accuracy.summarize(accuracy.field_errors(fields, ref), ports)
+        r["field_err_vs_peak"] = err_vs_peak(fields, ref, peak)
+        r["final_field_over_peak"] = max(float(np.linalg.norm(x)) for x in ref) / float(peak.max())
         r.update({"job": n, "grid": [edge] * 3, "time_steps": steps, "form": "fp32 served vs fp64 alone"})
         acc[kind] = r
         g.close()
