@@ -657,7 +657,10 @@ def footprint(dk, precision=FP32) -> int:
     if dk.gain:
         gid = dk.gain.get("gain_id", 5)
         ng = int((ids == gid).sum()) if ids is not None else cells
-        total += ng * ((24 if precision == FP32 else 25) * esz + 8)
+        if precision == FP32:  # segment-dense persistent words for every cell + list-layout transients
+            total += cells * 15 * 4 + ng * (9 * 4 + 8)
+        else:
+            total += ng * (25 * esz + 8)
     for p in dk.ports:
         npts = len(port_points(dk, p))
         nf = 0 if p.dft_freqs is None else len(p.dft_freqs)

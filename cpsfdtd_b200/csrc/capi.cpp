@@ -233,12 +233,16 @@ cps_status build_list(cps_grid *g, int id_match, int64_t *count, int64_t **d_cel
     return upload_raw(g, *d_seg, seg.data(), seg.size() * sizeof(int32_t));
 }
 
-// initial gain state, groups of 32 cells [group][word][32]: all zero (FP32
-// keeps population offsets) except FP64 N0 = N1 = 1 (FourLevelLaser.cpp:194-197)
+// initial gain state: all zero (FP32 keeps population offsets) except FP64
+// N0 = N1 = 1 (FourLevelLaser.cpp:194-197)
 cps_status gain_state_init(cps_grid *g)
 {
-    const int nw = g->fp32 ? kG32Words : kG64Words;
-    CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)gain_state_elems(g->g_n, nw) * g->esz, g->stream));
+    if (g->fp32) {
+        CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)g->elems * kGainPersist * sizeof(float), g->stream));
+        CK(cudaMemsetAsync(g->d_g_trans, 0, (size_t)gain_state_elems(g->g_n, kGainTrans) * sizeof(float), g->stream));
+    } else {
+        CK(cudaMemsetAsync(g->d_g_state, 0, (size_t)gain_state_elems(g->g_n, kG64Words) * sizeof(double), g->stream));
+    }
     if (!g->fp32 && g->g_n > 0) {
         launch_gain_init64((double *)g->d_g_state, g->g_n, g->stream);
         CK(cudaGetLastError());
@@ -412,6 +416,19 @@ cps_status ensure_tma(cps_grid *g)
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     REQUIRE(r == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for the IDs");
+    if (g->gain_on && g->fp32) {
+        // segment-dense gain words: {32 lanes, 15 words, segments, rows, planes}
+        const cuuint64_t nseg = (cuuint64_t)d.px / 32;
+        const cuuint64_t gdims[5] = {32, (cuuint64_t)kGainPersist, nseg, (cuuint64_t)(d.ny + 1), (cuuint64_t)(d.nz + 1)};
+        const cuuint64_t seg_b = (cuuint64_t)kGainPersist * 32 * sizeof(float);
+        const cuuint64_t gst[4] = {32 * sizeof(float), seg_b, nseg * seg_b, nseg * seg_b * (cuuint64_t)(d.ny + 1)};
+        const cuuint32_t gbox[5] = {32, (cuuint32_t)kGainPersist, 1, (cuuint32_t)by, 1};
+        const cuuint32_t ges[5] = {1, 1, 1, 1, 1};
+        r = enc(&g->tma.gain, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5, g->d_g_state, gdims, gst, gbox, ges,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        REQUIRE(r == CUDA_SUCCESS, CPS_E_CUDA, "cuTensorMapEncodeTiled failed for the gain words");
+    }
     g->tma_by = by;
     return CPS_OK;
 }
@@ -1151,10 +1168,15 @@ extern "C" cps_status cps_gain_init(cps_grid *g, const cps_gain_params *p)
     G.fpump = (float)G.pump_dt;
     g->gain_id = p->gain_id;
     if ((s = build_list(g, p->gain_id, &g->g_n, &g->d_g_cell, &g->d_g_seg, &g->d_g_segm))) return s;
-    const int nw = g->fp32 ? kG32Words : kG64Words;
-    if ((s = dalloc(g, &g->d_g_state, (size_t)gain_state_elems(g->g_n, nw) * g->esz))) return s;
+    if (g->fp32) {
+        if ((s = dalloc(g, &g->d_g_state, (size_t)g->elems * kGainPersist * sizeof(float)))) return s;
+        if ((s = dalloc(g, &g->d_g_trans, (size_t)gain_state_elems(g->g_n, kGainTrans) * sizeof(float)))) return s;
+    } else if ((s = dalloc(g, &g->d_g_state, (size_t)gain_state_elems(g->g_n, kG64Words) * sizeof(double)))) {
+        return s;
+    }
     if ((s = gain_state_init(g))) return s;
     g->gain_on = true;
+    g->tma_by = 0;  // the sweeps' tensor maps now include the gain words
     return CPS_OK;
 }
 
@@ -1999,16 +2021,23 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
     FLUSH_RECORDED(g);
     *ncells = g->g_n;
     if (!out) return CPS_OK;
-    const int nw = g->fp32 ? kG32Words : kG64Words;
-    const size_t n = (size_t)gain_state_elems(g->g_n, nw);
-    std::vector<double> st(n);
+    // FP32: the offsets n1 n2 n3 of each list cell gathered on the device;
+    // FP64: the list-layout state as it is
+    std::vector<double> st;
     if (g->fp32) {
-        std::vector<float> t(n);
-        CK(cudaMemcpyAsync(t.data(), g->d_g_state, n * 4, cudaMemcpyDeviceToHost, g->stream));
+        std::vector<float> t((size_t)g->g_n * 3);
+        float *d_out = nullptr;
+        cps_status s = dalloc(g, (void **)&d_out, t.size() * sizeof(float) + 16);
+        if (s) return s;
+        launch_gain_pops32((const float *)g->d_g_state, g->d_g_cell, g->g_n, d_out, g->stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(t.data(), d_out, t.size() * sizeof(float), cudaMemcpyDeviceToHost, g->stream));
         CK(cudaStreamSynchronize(g->stream));
-        for (size_t q = 0; q < n; ++q) st[q] = t[q];
+        dfree(g, d_out);
+        st.assign(t.begin(), t.end());
     } else {
-        CK(cudaMemcpyAsync(st.data(), g->d_g_state, n * 8, cudaMemcpyDeviceToHost, g->stream));
+        st.resize((size_t)gain_state_elems(g->g_n, kG64Words));
+        CK(cudaMemcpyAsync(st.data(), g->d_g_state, st.size() * 8, cudaMemcpyDeviceToHost, g->stream));
         CK(cudaStreamSynchronize(g->stream));
     }
     // device list is in device order (k, j, i); report in (i, j, k) order
@@ -2024,12 +2053,13 @@ extern "C" cps_status cps_gain_populations(cps_grid *g, double *out, int64_t *nc
     std::sort(ord.begin(), ord.end());
     const int64_t sc = kGainGroup;
     for (int64_t r = 0; r < g->g_n; ++r) {
-        const int64_t c = gain_base_index(ord[r].second, nw);
         double N[4];
         if (g->fp32) {
-            N[1] = 1.0 + st[12 * sc + c]; N[2] = st[13 * sc + c]; N[3] = st[14 * sc + c];
+            const int64_t c = ord[r].second * 3;
+            N[1] = 1.0 + st[c]; N[2] = st[c + 1]; N[3] = st[c + 2];
             N[0] = 2.0 - N[1] - N[2] - N[3];
         } else {
+            const int64_t c = gain_base_index(ord[r].second, kG64Words);
             for (int q = 0; q < 4; ++q) N[q] = st[(21 + q) * sc + c];
         }
         for (int q = 0; q < 4; ++q) out[r * 4 + q] = N[q];

@@ -88,6 +88,19 @@ __host__ __device__ constexpr int gain_words()
 {
     return sizeof(T) == 4 ? kG32Words : kG64Words;
 }
+// FP32 gain state, segment-dense: the 15 persistent words (Pa Pa1 Pb Pb1 x3,
+// n1 n2 n3) of every cell of the grid, [k][j][x-segment][word][32], so word w
+// of the cell at device index g is at gain_dense_index(g) + 32 w (g >> 5 is
+// the cell's (k, j, segment) row, g & 31 its lane).  A tile's gain words for a
+// plane are one box of a tensor map, staged with its fields.  The plain
+// path's transient words (Pa2 Pb2 E1) are kept apart, [group][9][32] by list
+// index.  FP64 grids keep all 25 words in the list layout below.
+constexpr int kGainPersist = 15;
+constexpr int kGainTrans = 9;
+__host__ __device__ inline int64_t gain_dense_index(int64_t g)
+{
+    return (g >> 5) * (int64_t)(kGainPersist * 32) + (g & 31);
+}
 // Gain state storage: the list cells in groups of 32, group q holding word w
 // of its cells at [q][w][32].  Word w of list cell c is then
 // state[gain_base_index(c, words) + w * kGainGroup]: one base per cell and a
@@ -180,7 +193,8 @@ struct GainView {
     const int64_t *cell;
     const int32_t *seg;
     const uint2 *segm;       // per (k, j, 32-wide x segment): list offset and the segment's gain-cell bit mask
-    T *state;                // [word][ncell]
+    T *state;                // FP64: list layout [group][word][32]; FP32: segment-dense persistent words
+    T *trans;                // FP32: the plain path's transient words, list layout [group][9][32]
     GainCoef c;
 };
 
@@ -236,6 +250,8 @@ template <typename T> void launch_dl(const FieldView<T> &f, const DlView<T> &d, 
 template <typename T> void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStream_t s);
 // initial gain state: FP64 N0 = N1 = 1 in every group (the rest zeroed by the caller)
 void launch_gain_init64(double *state, int64_t ncell, cudaStream_t s);
+// FP32 population offsets n1 n2 n3 of every list cell, [ncell][3]
+void launch_gain_pops32(const float *state, const int64_t *cell, int64_t ncell, float *out, cudaStream_t s);
 // three-level gain sites: which 0 polarisation, 1 E field, 2 populations, 3 all
 // three in order (kernels_three.cu, no FMA contraction); init: zero state, N0 = N_0
 template <typename T> void launch_three(const FieldView<T> &f, const ThreeView &t, int which, cudaStream_t s);

@@ -116,7 +116,8 @@ struct cps_grid {
     int64_t *d_g_cell = nullptr;
     int32_t *d_g_seg = nullptr;
     uint2 *d_g_segm = nullptr;
-    void *d_g_state = nullptr;
+    void *d_g_state = nullptr;  // FP32: segment-dense persistent words; FP64: all words, list layout
+    void *d_g_trans = nullptr;  // FP32: transient words of the plain path, list layout
     // three-level gain (FP64 state on both precisions)
     int ids_max = 0;              // largest material ID set
     bool three_on = false;
@@ -325,7 +326,7 @@ inline GainView<T> gain_view(const cps_grid *g)
     v.on = g->gain_on;
     if (!g->gain_on) return v;
     v.gain_id = g->gain_id; v.ncell = g->g_n; v.cell = g->d_g_cell; v.seg = g->d_g_seg; v.segm = g->d_g_segm;
-    v.state = (T *)g->d_g_state; v.c = g->gc;
+    v.state = (T *)g->d_g_state; v.trans = (T *)g->d_g_trans; v.c = g->gc;
     return v;
 }
 

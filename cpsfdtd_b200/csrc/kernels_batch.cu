@@ -102,7 +102,10 @@ __global__ void __launch_bounds__(32 * BY) k_e_batch(const BatchGrid<T> *__restr
             if (PML) stage_view(sp, B.p);
             if (DL) stage_view(sD, B.D);
             if (GAIN) stage_view(sG, B.G);
-            if (lead) acquire_maps(B.M, true);
+            if (lead) {
+                acquire_maps(B.M, true);
+                if (GAIN && sizeof(T) == 4) tensormap_acquire(&B.M.gain);
+            }
             __syncthreads();
             last = e.x;
         }
@@ -163,7 +166,7 @@ int occupancy(K kernel, int threads, int smem)
 template <typename T, int BY, bool PML, bool GAIN, bool DL>
 void e_batch(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nblocks, int *err, cudaStream_t s)
 {
-    using L = StageLayout<T, BY>;
+    using L = ELayout<T, BY, GAIN>;
     if (!smem_attr<k_e_batch<T, BY, PML, GAIN, DL>>(L::SMEM)) return;
     k_e_batch<T, BY, PML, GAIN, DL><<<nblocks, dim3(32, BY), L::SMEM, s>>>(grids, tiles, ntiles, err);
 }
@@ -187,30 +190,30 @@ void e_batch_by(const BatchGrid<T> *grids, const int4 *tiles, int ntiles, int nb
 template <typename T, int BY>
 void e_batch_attrs()
 {
-    using L = StageLayout<T, BY>;
-    smem_attr<k_e_batch<T, BY, false, false, false>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, true, false, false>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, false, false, true>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, true, false, true>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, false, true, false>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, true, true, false>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, false, true, true>>(L::SMEM);
-    smem_attr<k_e_batch<T, BY, true, true, true>>(L::SMEM);
+    constexpr int S = StageLayout<T, BY>::SMEM, SG = ELayout<T, BY, true>::SMEM;
+    smem_attr<k_e_batch<T, BY, false, false, false>>(S);
+    smem_attr<k_e_batch<T, BY, true, false, false>>(S);
+    smem_attr<k_e_batch<T, BY, false, false, true>>(S);
+    smem_attr<k_e_batch<T, BY, true, false, true>>(S);
+    smem_attr<k_e_batch<T, BY, false, true, false>>(SG);
+    smem_attr<k_e_batch<T, BY, true, true, false>>(SG);
+    smem_attr<k_e_batch<T, BY, false, true, true>>(SG);
+    smem_attr<k_e_batch<T, BY, true, true, true>>(SG);
 }
 
 template <typename T, int BY>
 int e_batch_occupancy(int cls)
 {
-    using L = StageLayout<T, BY>;
+    constexpr int S = StageLayout<T, BY>::SMEM, SG = ELayout<T, BY, true>::SMEM;
     switch (cls & 7) {
-    case 0: return occupancy(k_e_batch<T, BY, false, false, false>, 32 * BY, L::SMEM);
-    case 1: return occupancy(k_e_batch<T, BY, true, false, false>, 32 * BY, L::SMEM);
-    case 2: return occupancy(k_e_batch<T, BY, false, false, true>, 32 * BY, L::SMEM);
-    case 3: return occupancy(k_e_batch<T, BY, true, false, true>, 32 * BY, L::SMEM);
-    case 4: return occupancy(k_e_batch<T, BY, false, true, false>, 32 * BY, L::SMEM);
-    case 5: return occupancy(k_e_batch<T, BY, true, true, false>, 32 * BY, L::SMEM);
-    case 6: return occupancy(k_e_batch<T, BY, false, true, true>, 32 * BY, L::SMEM);
-    default: return occupancy(k_e_batch<T, BY, true, true, true>, 32 * BY, L::SMEM);
+    case 0: return occupancy(k_e_batch<T, BY, false, false, false>, 32 * BY, S);
+    case 1: return occupancy(k_e_batch<T, BY, true, false, false>, 32 * BY, S);
+    case 2: return occupancy(k_e_batch<T, BY, false, false, true>, 32 * BY, S);
+    case 3: return occupancy(k_e_batch<T, BY, true, false, true>, 32 * BY, S);
+    case 4: return occupancy(k_e_batch<T, BY, false, true, false>, 32 * BY, SG);
+    case 5: return occupancy(k_e_batch<T, BY, true, true, false>, 32 * BY, SG);
+    case 6: return occupancy(k_e_batch<T, BY, false, true, true>, 32 * BY, SG);
+    default: return occupancy(k_e_batch<T, BY, true, true, true>, 32 * BY, SG);
     }
 }
 

@@ -241,7 +241,8 @@ k_e_fused(FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc)
                 const int64_t base = G.seg[((int64_t)k * (d.ny + 1) + j) * nseg + blockIdx.x];
                 if (mine) {
                     const int64_t c = base + __popc(m & lanemask_lt()), sc = kGainGroup;
-                    T *st = G.state + gain_base_index(c, gain_words<T>());
+                    T *st = G.state + (sizeof(T) == 4 ? gain_dense_index(d.idx(i, j, k))
+                                                      : gain_base_index(c, kG64Words));
                     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
                     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
                     Pops<T> N;

@@ -179,7 +179,17 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
     const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (c >= G.ncell) return;
     const int64_t g = G.cell[c], sc = kGainGroup;
-    T *st = G.state + gain_base_index(c, gain_words<T>());
+    // persistent words (stride 32 in both layouts) and the transient words
+    // Pa2 Pb2 E1 (FP32: their own list-layout array)
+    T *st, *tr;
+    if (sizeof(T) == 4) {
+        st = G.state + gain_dense_index(g);
+        tr = G.trans + gain_base_index(c, kGainTrans);
+    } else {
+        st = G.state + gain_base_index(c, kG64Words);
+        tr = st;
+    }
+    auto tw = [&](int w) -> T & { return sizeof(T) == 4 ? tr[(w - kGainPersist) * sc] : st[w * sc]; };
     T *F[3] = {f.Ex, f.Ey, f.Ez};
     T E[3] = {F[0][g], F[1][g], F[2][g]};
     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
@@ -192,9 +202,9 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
         gain_load_n<T>(st, sc, N);
         gain_p_update<T>(G.c, N, E, Pa, Pa1, Pa2, Pb, Pb1, Pb2);
         for (int q = 0; q < 3; ++q) {
-            st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q]; st[(L::PA2 + q) * sc] = Pa2[q];
-            st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q]; st[(L::PB2 + q) * sc] = Pb2[q];
-            st[(L::E1 + q) * sc] = E[q];
+            st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q]; tw(L::PA2 + q) = Pa2[q];
+            st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q]; tw(L::PB2 + q) = Pb2[q];
+            tw(L::E1 + q) = E[q];
         }
     } else if (which == 1) {
         for (int q = 0; q < 3; ++q) F[q][g] = gain_e_corr<T>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
@@ -203,11 +213,20 @@ __global__ void k_gain(FieldView<T> f, GainView<T> G, int which)
         T E1[3];
         gain_load_n<T>(st, sc, N);
         for (int q = 0; q < 3; ++q) {
-            Pa2[q] = st[(L::PA2 + q) * sc]; Pb2[q] = st[(L::PB2 + q) * sc]; E1[q] = st[(L::E1 + q) * sc];
+            Pa2[q] = tw(L::PA2 + q); Pb2[q] = tw(L::PB2 + q); E1[q] = tw(L::E1 + q);
         }
         gain_n_update<T>(G.c, N, E, E1, Pa, Pa1, Pa2, Pb, Pb2);
         gain_store_n<T>(st, sc, N);
     }
+}
+
+// FP32 population offsets of each list cell for the host read-out
+__global__ void k_gain_pops32(const float *state, const int64_t *cell, int64_t ncell, float *out)
+{
+    const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const float *st = state + gain_dense_index(cell[c]);
+    for (int q = 0; q < 3; ++q) out[c * 3 + q] = st[(GainSite32::DN1 + q) * kGainGroup];
 }
 
 // FP64 initial populations N0 = N1 = 1 (words 21, 22 of each cell)
@@ -385,6 +404,12 @@ void launch_gain(const FieldView<T> &f, const GainView<T> &g, int which, cudaStr
         k_gain<T, GainSite64><<<cdiv(g.ncell, 128), 128, 0, s>>>(f, g, which);
     else
         k_gain<T, GainSite32><<<cdiv(g.ncell, 128), 128, 0, s>>>(f, g, which);
+}
+
+void launch_gain_pops32(const float *state, const int64_t *cell, int64_t ncell, float *out, cudaStream_t s)
+{
+    if (ncell <= 0) return;
+    k_gain_pops32<<<cdiv(ncell, 256), 256, 0, s>>>(state, cell, ncell, out);
 }
 
 void launch_gain_init64(double *state, int64_t ncell, cudaStream_t s)

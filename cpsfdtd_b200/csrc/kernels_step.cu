@@ -215,14 +215,10 @@ __device__ __forceinline__ void step_body(const StepMaps &M, const FieldView<T> 
     }
     const int ke0 = max(kb, 1);  // first plane of E updates
     constexpr bool GPRE = GAIN && sizeof(T) == 4;
+    // FP32 gain: the segment-dense words of plane k+1 requested during plane k
     GainRegs32 gcur{}, gnext{};
-    uint2 mcur{0u, 0u}, mnext{0u, 0u}, mnn{0u, 0u};
     if constexpr (GPRE) {
-        if (ke0 < ke) {
-            mcur = gain_segment(G, d, j, ke0, bx, rowok);
-            if (ke0 + 1 < ke) mnext = gain_segment(G, d, j, ke0 + 1, bx, rowok);
-            gain_fetch32(G, mcur, gcur);
-        }
+        if (ke0 < ke && rowok) gain_fetch32(G, d.idx(i, j, ke0), gcur);
     }
     const int hr = (ty + 1) * L::HW + tx + 4, er = (ty + 1) * L::EW + tx + 4, ir = (ty + 1) * L::IW + tx + 16;
     T hxm = 0, hym = 0;
@@ -239,10 +235,7 @@ __device__ __forceinline__ void step_body(const StepMaps &M, const FieldView<T> 
         HSum<T> hs{T(0), T(0), T(0)};
         if (TFSF && act_h) hs = h_corr_sum(hc, i, j, k);
         if constexpr (GPRE) {
-            if (eplane) {
-                mnn = k + 2 < ke ? gain_segment(G, d, j, k + 2, bx, rowok) : make_uint2(0u, 0u);
-                if (k + 1 < ke) gain_fetch32(G, mnext, gnext);
-            }
+            if (eplane && rowok && k + 1 < ke) gain_fetch32(G, d.idx(i, j, k + 1), gnext);
         }
         wait_plane(k + 1);
         const int q = k - ks;
@@ -284,10 +277,8 @@ __device__ __forceinline__ void step_body(const StepMaps &M, const FieldView<T> 
                     }
                 }
                 if constexpr (GPRE) {
-                    gain_apply32(G, mcur, gcur, ex, ey, ez);
+                    if (act && id == G.gain_id) gain_apply32(G, g, gcur, ex, ey, ez);
                     gcur = gnext;
-                    mcur = mnext;
-                    mnext = mnn;
                 } else if (GAIN && rowok) {
                     gain_warp(G, d, j, k, bx, act, id, ex, ey, ez);
                 }

@@ -147,7 +147,7 @@ template <typename T, int BY, int PM, bool DL, bool GAIN>
 int e_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
                  const GainView<T> &G, int kc, const TileBoxes &tb, int *err, cudaStream_t s)
 {
-    using L = StageLayout<T, BY>;
+    using L = StageLayout<T, BY, GAIN && sizeof(T) == 4>;
     const int blocks = tb.start[tb.n];
     if (blocks <= 0) return 0;
     if (!set_smem<k_e_tma<T, BY, PM, DL, GAIN>>(L::SMEM)) return 0;
@@ -172,17 +172,17 @@ int h_tma_launch(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, i
 template <typename T, int BY>
 void attrs_by()
 {
-    constexpr int S = StageLayout<T, BY>::SMEM;
+    constexpr int S = StageLayout<T, BY>::SMEM, SG = StageLayout<T, BY, sizeof(T) == 4>::SMEM;
     set_smem<k_h_tma<T, BY, 0>>(S);
     set_smem<k_h_tma<T, BY, 2>>(S);
     set_smem<k_e_tma<T, BY, 0, false, false>>(S);
-    set_smem<k_e_tma<T, BY, 0, false, true>>(S);
+    set_smem<k_e_tma<T, BY, 0, false, true>>(SG);
     set_smem<k_e_tma<T, BY, 0, true, false>>(S);
-    set_smem<k_e_tma<T, BY, 0, true, true>>(S);
+    set_smem<k_e_tma<T, BY, 0, true, true>>(SG);
     set_smem<k_e_tma<T, BY, 2, false, false>>(S);
     set_smem<k_e_tma<T, BY, 2, true, false>>(S);
-    set_smem<k_e_tma<T, BY, 1, false, true>>(S);
-    set_smem<k_e_tma<T, BY, 1, true, true>>(S);
+    set_smem<k_e_tma<T, BY, 1, false, true>>(SG);
+    set_smem<k_e_tma<T, BY, 1, true, true>>(SG);
 }
 
 template <typename T, int BY>

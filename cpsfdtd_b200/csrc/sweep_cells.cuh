@@ -280,7 +280,8 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
     const int64_t base = G.seg[((int64_t)k * (d.ny + 1) + j) * nseg + seg];
     if (!mine) return;
     const int64_t c = base + __popc(m & lanemask_lt()), sc = kGainGroup;
-    T *st = G.state + gain_base_index(c, gain_words<T>());
+    T *st = G.state + (sizeof(T) == 4 ? gain_dense_index(d.idx(seg * 32 + (int)(threadIdx.x & 31u), j, k))
+                                      : gain_base_index(c, kG64Words));
     T E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
     T Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
     Pops<T> N;
@@ -325,49 +326,56 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
 }
 
 
-// ---- FP32 gain with the state fetched one plane ahead.  The list offset and
-// the bit mask of a warp row's gain cells come from the segment table, so a
-// plane's state can be loaded before its fields arrive; the arithmetic is
-// gain_warp's.
+// ---- FP32 gain on the segment-dense layout: the 15 persistent words of the
+// cell at device index g are at gain_dense_index(g) + 32 w, for every cell of
+// the grid, so a plane's words can be requested (or staged by TMA) before its
+// fields and IDs arrive.  The arithmetic is gain_warp's.
 struct GainRegs32 {
     float pa[3], pa1[3], pb[3], pb1[3];
     float n[3];  // the population offsets N1 - 1, N2, N3
 };
 
-__device__ __forceinline__ uint2 gain_segment(const GainView<float> &G, const Dims &d, int j, int k, int seg,
-                                              bool rowok)
+// the words of the cell at device index g from global memory
+__device__ __forceinline__ void gain_fetch32(const GainView<float> &G, int64_t g, GainRegs32 &r)
 {
-    return rowok ? __ldg(&G.segm[((int64_t)k * (d.ny + 1) + j) * (d.px >> 5) + seg]) : make_uint2(0u, 0u);
-}
-
-__device__ __forceinline__ void gain_fetch32(const GainView<float> &G, uint2 m, GainRegs32 &r)
-{
-    const unsigned lane = threadIdx.x & 31u;
-    if (!((m.y >> lane) & 1u)) return;
     using L = GainSite32;
-    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = kGainGroup;
-    const float *st = G.state + gain_base_index(c, kG32Words);
+    const float *st = G.state + gain_dense_index(g);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        r.pa[q] = __ldg(st + (L::PA + q) * sc);
-        r.pa1[q] = __ldg(st + (L::PA1 + q) * sc);
-        r.pb[q] = __ldg(st + (L::PB + q) * sc);
-        r.pb1[q] = __ldg(st + (L::PB1 + q) * sc);
+        r.pa[q] = __ldg(st + (L::PA + q) * kGainGroup);
+        r.pa1[q] = __ldg(st + (L::PA1 + q) * kGainGroup);
+        r.pb[q] = __ldg(st + (L::PB + q) * kGainGroup);
+        r.pb1[q] = __ldg(st + (L::PB1 + q) * kGainGroup);
     }
-    r.n[0] = __ldg(st + L::DN1 * sc);
-    r.n[1] = __ldg(st + L::N2 * sc);
-    r.n[2] = __ldg(st + L::N3 * sc);
+    r.n[0] = __ldg(st + L::DN1 * kGainGroup);
+    r.n[1] = __ldg(st + L::N2 * kGainGroup);
+    r.n[2] = __ldg(st + L::N3 * kGainGroup);
 }
 
-// P -> E -> N at this lane's cell when it is a gain cell of the segment
-__device__ __forceinline__ void gain_apply32(const GainView<float> &G, uint2 m, const GainRegs32 &r, float &ex,
+// the words of a cell from a staged tile: word w at ws[32 w]
+__device__ __forceinline__ void gain_staged32(const float *ws, GainRegs32 &r)
+{
+    using L = GainSite32;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        r.pa[q] = ws[(L::PA + q) * 32];
+        r.pa1[q] = ws[(L::PA1 + q) * 32];
+        r.pb[q] = ws[(L::PB + q) * 32];
+        r.pb1[q] = ws[(L::PB1 + q) * 32];
+    }
+    r.n[0] = ws[L::DN1 * 32];
+    r.n[1] = ws[L::N2 * 32];
+    r.n[2] = ws[L::N3 * 32];
+}
+
+// P -> E -> N at a gain cell (device index g) from its words r; the new words
+// go to the dense state
+__device__ __forceinline__ void gain_apply32(const GainView<float> &G, int64_t g, const GainRegs32 &r, float &ex,
                                              float &ey, float &ez)
 {
-    const unsigned lane = threadIdx.x & 31u;
-    if (!((m.y >> lane) & 1u)) return;
     using L = GainSite32;
-    const int64_t c = (int64_t)m.x + __popc(m.y & lanemask_lt()), sc = kGainGroup;
-    float *st = G.state + gain_base_index(c, kG32Words);
+    float *st = G.state + gain_dense_index(g);
+    const int64_t sc = kGainGroup;
     float E[3] = {ex, ey, ez}, E1[3] = {ex, ey, ez};
     float Pa[3], Pa1[3], Pa2[3], Pb[3], Pb1[3], Pb2[3];
 #pragma unroll

@@ -10,10 +10,13 @@ namespace cps {
 // Tensor maps of the six field arrays and the ID array of one grid, x fastest:
 //   halo[c]: box 36 x (BY+1) x 1   own[c]: box 32 x BY x 1   id: box 32 x BY x 1
 // c = 0..5 for Ex Ey Ez Hx Hy Hz.
+//   gain: FP32 segment-dense gain words, dims {32 lanes, 15 words, segments,
+//         ny+1 rows, nz+1 planes}, box 32 x 15 x 1 x BY x 1 (grids with gain)
 struct TmaMaps {
     CUtensorMap halo[6];
     CUtensorMap own[6];
     CUtensorMap id;
+    CUtensorMap gain;
 };
 
 // Tensor maps of the one-pass step sweep over one field buffer, x fastest:
@@ -73,6 +76,17 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
         " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+        : "memory");
+}
+
+// 5-D tiled load (the segment-dense gain words), completion counted on bar
+__device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1, int c2,
+                                            int c3, int c4)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%3, %4, %5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4)
         : "memory");
 }
 

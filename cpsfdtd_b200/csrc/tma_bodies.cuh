@@ -43,16 +43,24 @@ constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
 __host__ __device__ constexpr int a128(int b) { return (b + 127) / 128 * 128; }
 
-template <typename T, int BY>
+// One stage: three halo tiles, three own tiles, the IDs and, for an FP32 E
+// sweep with gain (G), the tile's segment-dense gain words [row][word][32].
+template <typename T, int BY, bool G = false>
 struct StageLayout {
     static constexpr int HW = 36, HH = BY + 1, OW = 32, OH = BY;
     static constexpr int HALO_B = a128(HW * HH * (int)sizeof(T));
     static constexpr int OWN_B = a128(OW * OH * (int)sizeof(T));
     static constexpr int ID_B = a128(OW * OH);
-    static constexpr int STAGE_B = 3 * HALO_B + 3 * OWN_B + ID_B;
-    static constexpr uint32_t TX = 3 * HW * HH * sizeof(T) + 3 * OW * OH * sizeof(T) + OW * OH;
+    static constexpr int GAIN_OFF = 3 * HALO_B + 3 * OWN_B + ID_B;
+    static constexpr int GAIN_RAW = G ? 32 * kGainPersist * BY * 4 : 0;
+    static constexpr int STAGE_B = GAIN_OFF + a128(GAIN_RAW);
+    static constexpr uint32_t TX = 3 * HW * HH * sizeof(T) + 3 * OW * OH * sizeof(T) + OW * OH + GAIN_RAW;
     static constexpr int SMEM = kStages * STAGE_B + 128;
 };
+
+// the stage layout of an E sweep (FP32 with gain stages the gain words)
+template <typename T, int BY, bool GAIN>
+using ELayout = StageLayout<T, BY, GAIN && sizeof(T) == 4>;
 
 struct TileXYZ {
     int bx, by, bz;  // tile index along x (32 columns), y (BY rows), z (kc planes)
@@ -149,7 +157,9 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
                                            const DlView<T> &D, const GainView<T> &G, int kc, TileXYZ t,
                                            uint32_t &ctr, int *err, unsigned char *sm, uint64_t *full)
 {
-    using L = StageLayout<T, BY>;
+    // FP32 gain: the tile's gain words travel with its fields in every stage
+    constexpr bool GST = GAIN && sizeof(T) == 4;
+    using L = StageLayout<T, BY, GST>;
     const Dims d = f.d;
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * 32 + tx;
     const int x0 = t.bx * 32, y0 = t.by * BY;
@@ -169,6 +179,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         for (int c = 0; c < 3; ++c) tma_load_3d(b + c * L::HALO_B, &M.halo[3 + c], &full[s], x0 - 4, y0 - 1, k);
         for (int c = 0; c < 3; ++c) tma_load_3d(b + 3 * L::HALO_B + c * L::OWN_B, &M.own[c], &full[s], x0, y0, k);
         tma_load_3d(b + 3 * L::HALO_B + 3 * L::OWN_B, &M.id, &full[s], x0, y0, k);
+        if (GST) tma_load_5d(b + L::GAIN_OFF, &M.gain, &full[s], 0, 0, t.bx, y0, k);
     };
     if (tid == 0)
         for (int pl = 0; pl < kStages && k0 + pl < k1; ++pl) issue(pl, k0 + pl);
@@ -189,22 +200,9 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         psi_load_e(p, d, pc, i, j, k0, qc);
         if (k0 + 1 < k1) psi_load_e(p, d, pc, i, j, k0 + 1, qn);
     }
-    // FP32 gain: state of plane k fetched during plane k-1, segment table two planes ahead
-    constexpr bool GPRE = GAIN && sizeof(T) == 4;
-    GainRegs32 gcur{}, gnext{};
-    uint2 mcur{0u, 0u}, mnext{0u, 0u}, mnn{0u, 0u};
-    if constexpr (GPRE) {
-        mcur = gain_segment(G, d, j, k0, t.bx, rowok);
-        if (k0 + 1 < k1) mnext = gain_segment(G, d, j, k0 + 1, t.bx, rowok);
-        gain_fetch32(G, mcur, gcur);
-    }
     const int hr = (ty + 1) * L::HW + tx + 4, orow = ty * L::OW + tx;
     for (int k = k0, it = 0; k < k1; ++k, ++it) {
         if (PML && act && k + 2 < k1) psi_load_e(p, d, pc, i, j, k + 2, qnn);
-        if constexpr (GPRE) {
-            mnn = k + 2 < k1 ? gain_segment(G, d, j, k + 2, t.bx, rowok) : make_uint2(0u, 0u);
-            if (k + 1 < k1) gain_fetch32(G, mnext, gnext);
-        }
         const uint32_t q = c0 + (uint32_t)it;
         const int s = (int)(q % kStages);
         const bool ok = wait_stage(&full[s], (q / kStages) & 1u);
@@ -235,11 +233,13 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
             ey = aE * ey + bE * dHx_k * cEyx - bE * dHz_i * cEyz;
             ez = aE * ez + bE * dHy_i * cEzy - bE * dHx_j * cEzx;
         }
-        if constexpr (GPRE) {
-            gain_apply32(G, mcur, gcur, ex, ey, ez);
-            gcur = gnext;
-            mcur = mnext;
-            mnext = mnn;
+        if constexpr (GST) {
+            // the gain list holds interior cells only (act), with the gain ID
+            if (act && id == G.gain_id) {
+                GainRegs32 r;
+                gain_staged32((const float *)(b + L::GAIN_OFF) + ty * kGainPersist * 32 + tx, r);
+                gain_apply32(G, d.idx(i, j, k), r, ex, ey, ez);
+            }
         } else if (GAIN && rowok) {
             gain_warp(G, d, j, k, t.bx, act, id, ex, ey, ez);
         }
