@@ -55,7 +55,10 @@ struct StageLayout {
     static constexpr int GAIN_RAW = G ? 32 * kGainPersist * BY * 4 : 0;
     static constexpr int STAGE_B = GAIN_OFF + a128(GAIN_RAW);
     static constexpr uint32_t TX = 3 * HW * HH * sizeof(T) + 3 * OW * OH * sizeof(T) + OW * OH + GAIN_RAW;
-    static constexpr int SMEM = kStages * STAGE_B + 128;
+    // planes in flight: three when the stage carries gain words (more blocks
+    // per SM fit), kStages otherwise
+    static constexpr int NS = G ? 3 : kStages;
+    static constexpr int SMEM = NS * STAGE_B + 128;
 };
 
 // the stage layout of an E sweep (FP32 with gain stages the gain words)
@@ -87,11 +90,12 @@ __device__ __forceinline__ bool wait_stage(uint64_t *bar, uint32_t phase)
 // After a wait gave up: thread 0 waits (bounded) for the planes [pl0, pl1]
 // of the tile whose loads may still be in flight (the plane that gave up has
 // had its whole limit already)
+template <int NS = kStages>
 __device__ __forceinline__ void drain_stages(uint64_t *full, uint32_t c0, int pl0, int pl1)
 {
     for (int pl = pl0; pl <= pl1; ++pl) {
         const uint32_t q = c0 + (uint32_t)pl;
-        wait_stage(&full[q % kStages], (q / kStages) & 1u);
+        wait_stage(&full[q % NS], (q / NS) & 1u);
     }
 }
 
@@ -172,7 +176,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
     const int npl = k1 - k0;
     const uint32_t skew = tid == 0 ? wait_skew(err) : 0u;
     auto issue = [&](int pl, int k) {
-        const int s = (int)((c0 + (uint32_t)pl) % kStages);
+        const int s = (int)((c0 + (uint32_t)pl) % L::NS);
         unsigned char *b = sm + s * L::STAGE_B;
         fence_proxy_async_smem();  // the stage's previous contents were read through the generic proxy
         mbar_expect_tx(&full[s], L::TX + (pl == 0 ? skew : 0u));
@@ -182,7 +186,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         if (GST) tma_load_5d(b + L::GAIN_OFF, &M.gain, &full[s], 0, 0, t.bx, y0, k);
     };
     if (tid == 0)
-        for (int pl = 0; pl < kStages && k0 + pl < k1; ++pl) issue(pl, k0 + pl);
+        for (int pl = 0; pl < L::NS && k0 + pl < k1; ++pl) issue(pl, k0 + pl);
     const int ic = act ? i : 1, jc = rowok ? j : 1;
     const StretchView<T> &sv = f.s;
     const T cEyz = sv.cEyz[ic], cEzy = sv.cEzy[ic], cExz = sv.cExz[jc], cEzx = sv.cEzx[jc];
@@ -204,12 +208,12 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
     for (int k = k0, it = 0; k < k1; ++k, ++it) {
         if (PML && act && k + 2 < k1) psi_load_e(p, d, pc, i, j, k + 2, qnn);
         const uint32_t q = c0 + (uint32_t)it;
-        const int s = (int)(q % kStages);
-        const bool ok = wait_stage(&full[s], (q / kStages) & 1u);
+        const int s = (int)(q % L::NS);
+        const bool ok = wait_stage(&full[s], (q / L::NS) & 1u);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
                 atomicExch(err, 1);
-                drain_stages(full, c0, it + 1, min(it + kStages - 1, npl - 1));
+                drain_stages<L::NS>(full, c0, it + 1, min(it + L::NS - 1, npl - 1));
             }
             return false;
         }
@@ -254,7 +258,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
         qc = qn;
         qn = qnn;
         __syncthreads();
-        if (tid == 0 && k + kStages < k1) issue(it + kStages, k + kStages);
+        if (tid == 0 && k + L::NS < k1) issue(it + L::NS, k + L::NS);
     }
     ctr = c0 + (uint32_t)(k1 - k0);
     return true;
