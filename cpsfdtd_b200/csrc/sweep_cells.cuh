@@ -305,13 +305,14 @@ __device__ __forceinline__ void gain_warp(const GainView<T> &G, const Dims &d, i
 #pragma unroll
     for (int q = 0; q < 3; ++q) E[q] = gain_e_corr<T>(G.c, E[q], Pa[q], Pa1[q], Pb[q], Pb1[q]);
     gain_n_update<T>(G.c, N, E, E1, Pa, Pa1, Pa2, Pb, Pb2);
+    // the transient words (Pa2 Pb2 E1) are not stored: only the plain path's
+    // separate routines read them, after its own polarisation routine wrote them
     if (sizeof(T) == 8) {
         using L = GainSite64;
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
-            st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q]; st[(L::PA2 + q) * sc] = Pa2[q];
-            st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q]; st[(L::PB2 + q) * sc] = Pb2[q];
-            st[(L::E1 + q) * sc] = E1[q];
+            st[(L::PA + q) * sc] = Pa[q]; st[(L::PA1 + q) * sc] = Pa1[q];
+            st[(L::PB + q) * sc] = Pb[q]; st[(L::PB1 + q) * sc] = Pb1[q];
         }
     } else {
         using L = GainSite32;
