@@ -87,6 +87,7 @@ struct cps_batch {
     bool dirty = true;
     // configuration
     int by = 4, kc = 16, persistent = 2, graph = 1;  // per-member launches: fastest on the measured mixes
+    int kch = 0;  // planes per tile of the per-member H sweeps (0: kc)
     // device tables (owned)
     std::vector<void *> owned;
     void *d_grids = nullptr;
@@ -399,7 +400,8 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
         per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
-            n += launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc}, b->d_err, ms);
+            n += launch_h_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), FusedShape{b->by, b->kc, b->kch}, b->d_err,
+                                 ms);
         });
         launch_inject_batch<T>(G, b->d_inj[1], b->ninj[1], 1, s, st);
         for (int c = 0; c < 8; ++c)
@@ -542,6 +544,14 @@ bool cache_lookup(const char *path, const std::string &key, int *by, int *kc, in
 }
 
 }  // namespace
+
+void cps::batch_set_h_planes(cps_batch *b, int kch)
+{
+    if (b->kch != kch) {
+        b->kch = kch;
+        b->dirty = true;  // captured chunks launch the per-member H sweeps with it
+    }
+}
 
 // clears a batch's device error word (the grid reset of a grid stepped
 // through its internal one-grid batch)

@@ -266,8 +266,9 @@ void launch_sources(const FieldView<T> &f, int nsrc, const int64_t *idx, const i
 
 // Fused path (kernels_fused.cu): 2.5D z-marching sweeps.
 struct FusedShape {
-    int by;   // rows per block (block = 32 x by threads)
-    int kc;   // planes per block along z
+    int by;       // rows per block (block = 32 x by threads)
+    int kc;       // planes per block along z (E sweep; H sweep too when kch is 0)
+    int kch = 0;  // planes per block of the TMA H sweep (0: kc)
 };
 template <typename T>
 void launch_h_fused(const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, cudaStream_t s);

@@ -218,7 +218,8 @@ template <typename T>
 int launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
                  cudaStream_t s)
 {
-    return sh.by == 4 ? h_tma_by<T, 4>(M, f, p, sh.kc, err, s) : h_tma_by<T, 8>(M, f, p, sh.kc, err, s);
+    const int kc = sh.kch > 0 ? sh.kch : sh.kc;
+    return sh.by == 4 ? h_tma_by<T, 4>(M, f, p, kc, err, s) : h_tma_by<T, 8>(M, f, p, kc, err, s);
 }
 
 template <typename T>
