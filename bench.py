@@ -94,6 +94,8 @@ def parse():
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving leg (0: skip)")
     ap.add_argument("--serve-step-scale", type=float, default=1.0,
                     help="job step counts are the log-uniform [500, 20000] draws divided by this")
+    ap.add_argument("--serve-fp64-steps", type=int, default=500,
+                    help="steps of each job timed on the FP64 plain path (scaled to the job's length; 0: skip)")
     ap.add_argument("--serve-tile", default="",
                     help="batch tile of the serving loop as rows,planes,mode (empty: the library default)")
     ap.add_argument("--serve-load", type=float, default=2.0,
@@ -629,7 +631,7 @@ def ensemble(args, local, dist):
     tile = list(b.get_tile())
     b.close()
 
-    def loop(path, steps):
+    def loop(path, steps, grids=grids):
         # one grid after another on the device: each grid's stream waits for
         # the previous grid's last launch; events on the current stream bracket
         # the chain
@@ -655,13 +657,27 @@ def ensemble(args, local, dist):
     fused = loop(cps.FUSED, args.ens_loop_steps)
     for g in grids:
         g.close()
+    # the plain form proper: FP64, one grid per launch (the parity form)
+    plain64 = None
+    if not args.no_fp64:
+        g64 = [cps.Grid.from_deck(decks.config4_member(nx, ny, nz, seed=i, steps=5000, nfreq=32), cps.FP64,
+                                  device=local) for i, (nx, ny, nz) in enumerate(shapes)]
+        loop(cps.PLAIN, 2, g64)
+        plain64 = loop(cps.PLAIN, args.ens_loop_steps, g64)
+        for g in g64:
+            g.close()
     return {"workload": f"{args.ens_grids} disordered-crystal realizations, edges U{{64,80,96,112,128}} per axis, "
                         "CPML 8, four-level gain, Ez seed pulse, 32-freq FP64 spherical-port DFT; FP32 fields",
             "grids": args.ens_grids, "cells": int(cells), "metric": "Gcell-upd/s", "value": batched,
             "steps_timed": args.ens_steps, "ms": ms, "tile": tile,
             "plain_one_grid_per_launch": plain, "fused_one_grid_per_launch": fused,
+            "plain_fp64_one_grid_per_launch": plain64,
             "speedup_vs_plain_loop": batched / plain if plain else None,
             "speedup_vs_fused_loop": batched / fused if fused else None,
+            "speedup_vs_plain_fp64_loop": batched / plain64 if plain64 else None,
+            "arms": "batched: FP32 fields (the chosen form, within 1e-4 of FP64); plain and fused loops: the same "
+                    "FP32 grids one grid per launch; plain FP64 loop: the parity form (FP64, one kernel per "
+                    "reference routine, one grid per launch) on the same decks",
             "gpu_launches": int(launches), "setup_s": setup_s, "autotune_s": tune_s,
             "autotune_steps": tuned_steps, "loop_steps_per_grid": args.ens_loop_steps,
             "timing": "all arms: CUDA events around the whole loop on the device (the loops' grids stepped one "
@@ -696,6 +712,21 @@ def serve_deck(kind, edge, steps, seed):
     return decks.config3(n=edge, steps=steps, seed=seed, nfreq=32)
 
 
+def trim_device_pool(local):
+    """Hand the memory that the library's grids returned to the device's
+    default pool (it keeps freed blocks for the next grid) back to the driver,
+    so that the free-memory figure counts it."""
+    import torch
+    torch.cuda.synchronize(local)
+    try:
+        from cuda.bindings import runtime as rt
+        err, pool = rt.cudaDeviceGetDefaultMemPool(local)
+        if err == rt.cudaError_t.cudaSuccess:
+            rt.cudaMemPoolTrimTo(pool, 0)
+    except ImportError:
+        pass
+
+
 def serving(args, local):
     """Served job stream through the library's serving loop (Poisson arrivals
     offered at --serve-load times a 20 Gcell-upd/s service rate, admission
@@ -713,6 +744,7 @@ def serving(args, local):
     arrivals = np.cumsum(rng.exponential(mean_gap, size=len(jobs)))
     arrivals -= arrivals[0]
     budget = 180 * 10 ** 9
+    trim_device_pool(local)
     free, total = torch.cuda.mem_get_info(local)
     budget = min(budget, int(free * 0.9))
     tile = tuple(int(v) for v in args.serve_tile.split(",")) if args.serve_tile else None
@@ -766,11 +798,46 @@ def serving(args, local):
         g.sync()
         g.close()
         service.append(time.perf_counter() - ts)
-    finish, plain_lat = 0.0, []
-    for a, sv in zip(arrivals, service):
-        finish = max(finish, a) + sv
-        plain_lat.append(finish - a)
-    plain_lat.sort()
+    def queued(service):
+        finish, out = 0.0, []
+        for a, sv in zip(arrivals, service):
+            finish = max(finish, a) + sv
+            out.append(finish - a)
+        return finish, sorted(out)
+
+    finish, plain_lat = queued(service)
+
+    # the plain form proper (FP64, one grid per launch): set-up and spectrum
+    # read-out measured per job, stepping timed over the job's first
+    # --serve-fp64-steps steps and scaled to its step count
+    plain64 = None
+    if not args.no_fp64 and args.serve_fp64_steps > 0:
+        service64 = []
+        for kind, edge, steps, seed in jobs:
+            dk = serve_deck(kind, edge, steps, seed)
+            torch.cuda.synchronize()
+            ts = time.perf_counter()
+            g = cps.Grid.from_deck(dk, cps.FP64, device=local)
+            g.sync()
+            t1 = time.perf_counter()
+            n = min(steps, args.serve_fp64_steps)
+            g.step(n, cps.PLAIN)
+            g.sync()
+            t2 = time.perf_counter()
+            for p in range(len(g.ports)):
+                if g.ports[p][2] > 0:
+                    g.port_dft(p, raw=True)
+            g.sync()
+            t3 = time.perf_counter()
+            g.close()
+            service64.append((t1 - ts) + (t2 - t1) * steps / n + (t3 - t2))
+        finish64, lat64 = queued(service64)
+        plain64 = {"jobs_per_s": len(jobs) / max(finish64, 1e-9),
+                   "gcell_upd_per_s": float(sum(work)) / sum(service64) / 1e9,
+                   "latency_p50_s": float(np.percentile(lat64, 50)),
+                   "latency_p99_s": float(np.percentile(lat64, 99)),
+                   "timing": f"host clock; set-up and read-out measured, stepping timed over each job's first "
+                             f"{args.serve_fp64_steps} steps and scaled to its step count"}
 
     # accuracy of the served results against FP64 runs alone
     acc = {}
@@ -810,6 +877,9 @@ def serving(args, local):
                                     "gcell_upd_per_s": cells_total / sum(service) / 1e9,
                                     "latency_p50_s": pct(plain_lat, 50), "latency_p99_s": pct(plain_lat, 99)},
             "speedup_gcell_vs_plain": (cells_total / span) / (cells_total / sum(service)),
+            "plain_fp64_one_at_a_time": plain64,
+            "speedup_gcell_vs_plain_fp64": (cells_total / span) / (plain64["gcell_upd_per_s"] * 1e9)
+            if plain64 else None,
             "accuracy": acc,
             "timing": "host clock: job latency = completion - arrival, including deck generation and grid "
                       "set-up; plain latencies from measured service times queued in arrival order"}
