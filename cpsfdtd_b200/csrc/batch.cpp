@@ -322,9 +322,10 @@ cps_status rebuild_T(cps_batch *b)
             if (P.nfreq > 0 && P.npts > 0) {
                 tab_size.push_back({pi, (size_t)2 * kMaxRing * P.nfreq * sizeof(double2)});
                 for (int q0 = 0; q0 < kMaxRing * P.nfreq; q0 += 256) phasor.push_back(make_int2(pi, q0));
-                for (int fb = 0; fb < cdiv_i(P.nfreq, 64); ++fb)
+                const int ft = dft_freq_tile(P.nfreq), pt = dft_point_tile(P.nfreq);
+                for (int fb = 0; fb < cdiv_i(P.nfreq, ft); ++fb)
                     for (int ci = 0; ci < P.ncomp; ++ci)
-                        for (int pb = 0; pb < cdiv_i(P.npts, 64); ++pb) dft.push_back(make_int4(pi, pb, ci, fb));
+                        for (int pb = 0; pb < cdiv_i(P.npts, pt); ++pb) dft.push_back(make_int4(pi, pb, ci, fb));
             }
             hp.push_back(bp);
         }

@@ -52,6 +52,12 @@ struct BatchPort {
 };
 
 constexpr int kMaxRing = 64;  // samples per port ring = longest chunk
+
+// DFT contraction tile of a port: 64 frequencies x 64 points per block, or
+// 32 frequencies x 128 points when the port transforms at most 32 (no block
+// then spends half its threads on frequencies the port does not have)
+__host__ __device__ constexpr int dft_freq_tile(int nfreq) { return nfreq <= 32 ? 32 : 64; }
+__host__ __device__ constexpr int dft_point_tile(int nfreq) { return nfreq <= 32 ? 128 : 64; }
 constexpr int kInjThreads = 128;                // threads of a batched injection block
 constexpr int kInjPerBlock = 2 * kInjThreads;   // TF/SF targets per injection block entry
 

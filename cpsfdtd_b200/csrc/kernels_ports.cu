@@ -58,30 +58,39 @@ __global__ void k_phasors(const double *omega, int nfreq, int nslots, int64_t n_
     phasor_entry(omega, nfreq, nslots, n_first, dt, q, tab);
 }
 
-// Contraction of one flush: a block of 256 threads covers 64 points x 64
-// frequencies of one component; thread (tp, tf) owns points p0 + 16a + tp
-// (a = 0..3) at frequencies f0 + 4tf + b (b = 0..3), so neighbouring lanes
-// touch neighbouring points in shared memory and in the accumulators.  The
-// block's samples [slots][64] and phasors [slots][64] are staged in shared
-// memory; each thread loads its 16 FP64 accumulator pairs, adds the samples
-// one slot at a time (acc_re += s cos, acc_im -= s sin, FP64 fused
-// multiply-adds) and stores them back.
-constexpr int kPT = 64, kFT = 64, kMaxSlots = 64;
-constexpr size_t kDftSmem(size_t esz) { return (esz * kPT + sizeof(double2) * kFT) * kMaxSlots; }
-
-template <typename T>
-__device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
-                                          int comp, int ci, int p0, int f0, double *acc, unsigned char *sh_raw)
+// Contraction of one flush: a block of 256 threads covers PT points x FT
+// frequencies of one component (64 x 64, or 128 x 32 for ports with at most
+// 32 frequencies); thread (tp, tf), tp < PT/4, tf < FT/4, owns points
+// p0 + (PT/4)a + tp (a = 0..3) at frequencies f0 + 4tf + b (b = 0..3), so
+// neighbouring lanes touch neighbouring points in shared memory and in the
+// accumulators.  The block's samples [slots][PT] and phasors [slots][FT] are
+// staged in shared memory; each thread loads its 16 FP64 accumulator pairs,
+// adds the samples one slot at a time (acc_re += s cos, acc_im -= s sin,
+// FP64 fused multiply-adds) and stores them back.  Every accumulator sees
+// the same operations in the same order whatever the tile.
+constexpr int kMaxSlots = 64;
+// shared memory of either tile: samples [slots][PT] + phasors [slots][FT]
+constexpr size_t kDftSmem(size_t esz)
 {
-    T *ss = reinterpret_cast<T *>(sh_raw);                                          // [nslots][kPT]
-    double2 *sp = reinterpret_cast<double2 *>(sh_raw + sizeof(T) * kMaxSlots * kPT);  // [nslots][kFT]
-    const int tid = threadIdx.x, tp = tid & 15, tf = tid >> 4;
-    for (int q = tid; q < nslots * kPT; q += blockDim.x) {
-        const int t = q / kPT, pl = q - t * kPT, p = p0 + pl;
+    return (esz * 64 + sizeof(double2) * 64) * kMaxSlots > (esz * 128 + sizeof(double2) * 32) * kMaxSlots
+               ? (esz * 64 + sizeof(double2) * 64) * kMaxSlots
+               : (esz * 128 + sizeof(double2) * 32) * kMaxSlots;
+}
+
+template <typename T, int FT>
+__device__ __forceinline__ void dft_tile(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
+                                         int comp, int ci, int p0, int f0, double *acc, unsigned char *sh_raw)
+{
+    constexpr int TF = FT / 4, TP = 256 / TF, PT = 4 * TP;
+    T *ss = reinterpret_cast<T *>(sh_raw);                                          // [nslots][PT]
+    double2 *sp = reinterpret_cast<double2 *>(sh_raw + sizeof(T) * kMaxSlots * PT);  // [nslots][FT]
+    const int tid = threadIdx.x, tp = tid % TP, tf = tid / TP;
+    for (int q = tid; q < nslots * PT; q += blockDim.x) {
+        const int t = q / PT, pl = q - t * PT, p = p0 + pl;
         ss[q] = p < npts ? ring[((int64_t)t * 6 + comp) * npts + p] : T(0);
     }
-    for (int q = tid; q < nslots * kFT; q += blockDim.x) {
-        const int t = q / kFT, fl = q - t * kFT, f = f0 + fl;
+    for (int q = tid; q < nslots * FT; q += blockDim.x) {
+        const int t = q / FT, fl = q - t * FT, f = f0 + fl;
         sp[q] = f < nfreq ? tab[(int64_t)t * nfreq + f] : make_double2(0.0, 0.0);
     }
     double re[4][4], im[4][4];
@@ -91,7 +100,7 @@ __device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, c
         const double *ar = acc + ((int64_t)(ci * nfreq + min(f, nfreq - 1)) * 2) * npts;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const int p = p0 + a * 16 + tp;
+            const int p = p0 + a * TP + tp;
             const bool ok = f < nfreq && p < npts;
             re[a][b] = ok ? ar[p] : 0.0;
             im[a][b] = ok ? ar[npts + p] : 0.0;
@@ -101,10 +110,10 @@ __device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, c
     for (int t = 0; t < nslots; ++t) {
         double sv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) sv[a] = (double)ss[t * kPT + a * 16 + tp];
+        for (int a = 0; a < 4; ++a) sv[a] = (double)ss[t * PT + a * TP + tp];
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-            const double2 w = sp[t * kFT + tf * 4 + b];
+            const double2 w = sp[t * FT + tf * 4 + b];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 re[a][b] = __fma_rn(sv[a], w.x, re[a][b]);
@@ -119,12 +128,23 @@ __device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, c
         double *ar = acc + ((int64_t)(ci * nfreq + f) * 2) * npts;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const int p = p0 + a * 16 + tp;
+            const int p = p0 + a * TP + tp;
             if (p >= npts) continue;
             ar[p] = re[a][b];
             ar[npts + p] = im[a][b];
         }
     }
+}
+
+// block (pb, fb) of a port's contraction, with the port's tile
+template <typename T>
+__device__ __forceinline__ void dft_block(const T *ring, int npts, int nslots, const double2 *tab, int nfreq,
+                                          int comp, int ci, int pb, int fb, double *acc, unsigned char *sh_raw)
+{
+    if (dft_freq_tile(nfreq) == 32)
+        dft_tile<T, 32>(ring, npts, nslots, tab, nfreq, comp, ci, pb * 128, fb * 32, acc, sh_raw);
+    else
+        dft_tile<T, 64>(ring, npts, nslots, tab, nfreq, comp, ci, pb * 64, fb * 64, acc, sh_raw);
 }
 
 template <typename T>
@@ -134,7 +154,7 @@ __global__ void __launch_bounds__(256, 2) k_dft(const T *ring, int npts, int nsl
     extern __shared__ __align__(16) unsigned char sh_raw[];
     const int ci = blockIdx.y, comp = comps[ci];
     dft_block<T>(ring, npts, nslots, tab + (comp >= 3 ? (int64_t)nslots * nfreq : 0), nfreq, comp, ci,
-                 blockIdx.x * kPT, blockIdx.z * kFT, acc, sh_raw);
+                 blockIdx.x, blockIdx.z, acc, sh_raw);
 }
 
 // batched forms over the ports of many grids
@@ -197,7 +217,7 @@ __global__ void __launch_bounds__(256, 2) k_dft_batch(const BatchPort<T> *__rest
     const BatchPort<T> &P = ports[e.x];
     const int comp = P.comps[e.z];
     dft_block<T>(P.ring, P.npts, nslots, P.tab + (comp >= 3 ? (int64_t)kMaxRing * P.nfreq : 0), P.nfreq, comp, e.z,
-                 e.y * kPT, e.w * kFT, P.acc, sh_raw);
+                 e.y, e.w, P.acc, sh_raw);
 }
 
 // flux[f] = 0.5 * Re sum_p (A_p conj(B_p) - C_p conj(D_p)) * dA over the
@@ -277,7 +297,7 @@ void launch_port_dft(const T *ring, int npts, int nslots, int64_t n_first, doubl
     if (npts <= 0 || nslots <= 0 || nfreq <= 0 || ncomp <= 0) return;
     double2 *tab = reinterpret_cast<double2 *>(scratch_phasor);
     k_phasors<<<cdiv((int64_t)nslots * nfreq, 256), 256, 0, s>>>(omega, nfreq, nslots, n_first, dt, tab);
-    dim3 grid(cdiv(npts, kPT), ncomp, cdiv(nfreq, kFT));
+    dim3 grid(cdiv(npts, dft_point_tile(nfreq)), ncomp, cdiv(nfreq, dft_freq_tile(nfreq)));
     if (!kernel_smem<k_dft<T>>((int)kDftSmem(sizeof(T)))) return;
     k_dft<T><<<grid, 256, kDftSmem(sizeof(T)), s>>>(ring, npts, nslots, tab, nfreq, comps, acc);
 }

@@ -50,6 +50,8 @@ CASES = {"c1": lambda: decks.config1(n=32, steps=120),
          "c2_drude": _c2_drude,
          "c3_three": _c3_three,
          "c2": lambda: decks.config2(n=48, steps=100, nfreq=8),
+         # more frequencies than one 64-wide DFT tile holds (a ragged second tile)
+         "c2_70freq": lambda: decks.config2(n=40, steps=60, nfreq=70),
          "c2_cw": gc.c2_cw,
          "c3": lambda: decks.config3(n=40, steps=100, nfreq=4),
          "shapes": gc.shapes_pec}
@@ -229,3 +231,26 @@ def test_port_flux_matches_oracle(prec, oracle_runs):
         assert err <= tol, f"port {n} ({normal}) flux error {err:.3e}"
         assert np.array_equal(g.port_flux(n, normal), got)
     g.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "fp32"])
+def test_dft_tiles_agree_bit_for_bit(prec):
+    """Ports with at most 32 frequencies are contracted in 128-point x
+    32-frequency tiles, others in 64 x 64 tiles; every accumulator sees the
+    same operations either way.  The same ports with 32 frequencies and with
+    those 32 plus one more give identical accumulators for the 32."""
+    import cpsfdtd_b200 as cps
+    base = decks.config2(n=40, steps=70, nfreq=32)
+    out = []
+    for extra in (False, True):
+        dk = decks.config2(n=40, steps=70, nfreq=32)
+        for p, q in zip(dk.ports, base.ports):
+            f = np.asarray(q.dft_freqs, dtype=np.float64)
+            p.dft_freqs = np.concatenate([f, [f[-1] * 1.01]]) if extra else f.copy()
+        g = cps.Grid.from_deck(dk, prec, device=0)
+        g.step(dk.nsteps, cps.FUSED)
+        out.append([np.array(g.port_dft(n)[:, :, :32, :]) for n, p in enumerate(dk.ports) if p.dft_freqs is not None])
+        g.close()
+    assert len(out[0]) == len(out[1]) > 0
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
