@@ -411,7 +411,7 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
             n += launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
-                            FusedShape{b->by, b->kc}, b->d_err, ms);
+                            FusedShape{b->by, b->kc}, b->d_err, ms, &g->lane);
         });
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);

@@ -663,7 +663,7 @@ cps_status step_T(cps_grid *g, int nsteps, int path)
             if (timed) cudaEventRecord(g->ev[g->ev_used + 1], g->stream);
             op_inject<T>(g, 1, (double)n, CPS_FACE_ALL);
             if (timed) cudaEventRecord(g->ev[g->ev_used + 2], g->stream);
-            if (use_tma) g->launches += launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream);
+            if (use_tma) g->launches += launch_e_tma<T>(g->tma, f, p, D, G, g->shape, g->d_err, g->stream, &g->lane);
             else launch_e_fused<T>(f, p, D, G, g->shape, g->stream), g->launches++;
             if (g->three_on) {
                 launch_three<T>(f, three_view(g), 3, g->stream);
@@ -741,6 +741,10 @@ extern "C" cps_status cps_grid_create(const cps_grid_desc *desc, cps_grid **out)
     cudaError_t e = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); delete g; return CPS_E_CUDA; }
     g->own_stream = true;
+    e = cudaStreamCreateWithFlags(&g->lane.s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->lane.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g->lane.join, cudaEventDisableTiming);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); cps_grid_destroy(g); return CPS_E_CUDA; }
     cps_status s = CPS_OK;
     for (int c = 0; c < 6 && !s; ++c) s = dalloc(g, &g->F[c], (size_t)g->elems * g->esz);
     if (!s) s = dalloc(g, (void **)&g->d_id, (size_t)g->elems);
@@ -772,6 +776,10 @@ extern "C" cps_status cps_grid_destroy(cps_grid *g)
     g->owned.clear();
     if (g->stream) cudaStreamSynchronize(g->stream);
     for (auto &e : g->ev) cudaEventDestroy(e);
+    if (g->lane.s) cudaStreamSynchronize(g->lane.s);
+    if (g->lane.fork) cudaEventDestroy(g->lane.fork);
+    if (g->lane.join) cudaEventDestroy(g->lane.join);
+    if (g->lane.s) cudaStreamDestroy(g->lane.s);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     delete g;
     return CPS_OK;
@@ -1742,7 +1750,8 @@ cps_status run_fused_T(cps_grid *g, const std::vector<RecOp> &ops)
             break;
         case kOpEBulk:
             if (use_tma)
-                g->launches += launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream);
+                g->launches += launch_e_tma<T>(g->tma, f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->d_err, g->stream,
+                                             &g->lane);
             else launch_e_fused<T>(f, p, dl_view<T>(g), gain_view<T>(g), g->shape, g->stream), g->launches++;
             if (g->three_on) {
                 launch_three<T>(f, three_view(g), 3, g->stream);

@@ -270,6 +270,14 @@ struct FusedShape {
     int kc;       // planes per block along z (E sweep; H sweep too when kch is 0)
     int kch = 0;  // planes per block of the TMA H sweep (0: kc)
 };
+// A second stream of a grid with a fork and a join event: work that does not
+// depend on a sweep (the Drude-Lorentz cell pass beside the E sweep) runs on
+// it between the fork and the join, which a stream capture records as graph
+// edges.  Created with the grid, outside any capture.
+struct SideLane {
+    cudaStream_t s = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
 template <typename T>
 void launch_h_fused(const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, cudaStream_t s);
 template <typename T>
@@ -285,9 +293,12 @@ namespace cps {
 template <typename T>
 int launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, FusedShape sh, int *err,
                  cudaStream_t s);
+// With a side lane, the Drude-Lorentz cell pass runs on it beside the E sweep
+// (the sweep leaves the ID-2 cells, their E and their psi alone, and both
+// read only H and the cells' own old E); the call returns after the join.
 template <typename T>
 int launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s);
+                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s, const SideLane *lane = nullptr);
 // set the shared-memory attributes of every TMA sweep kernel (call outside captures)
 template <typename T>
 void tma_attributes();

@@ -82,6 +82,7 @@ struct cps_grid {
     size_t esz = 8;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cps::SideLane lane;  // the Drude-Lorentz cell pass beside the E sweep
     Dims d{};
     int64_t elems = 0;  // device elements per field array
     void *F[6] = {};

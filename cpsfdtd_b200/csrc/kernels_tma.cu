@@ -224,15 +224,26 @@ int launch_h_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, F
 
 template <typename T>
 int launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const DlView<T> &D,
-                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s)
+                 const GainView<T> &G, FusedShape sh, int *err, cudaStream_t s, const SideLane *lane)
 {
-    int n = sh.by == 4 ? e_tma_by<T, 4>(M, f, p, D, G, sh.kc, err, s) : e_tma_by<T, 8>(M, f, p, D, G, sh.kc, err, s);
-    if (D.on && D.ncell > 0) {
-        if (p.on) k_dl_cells<T, true><<<cdiv(D.ncell, 128), 128, 0, s>>>(f, p, D);
-        else k_dl_cells<T, false><<<cdiv(D.ncell, 128), 128, 0, s>>>(f, p, D);
-        ++n;
+    const bool dl = D.on && D.ncell > 0;
+    const bool beside = dl && lane && lane->s;
+    cudaStream_t ds = s;
+    if (beside) {
+        cudaEventRecord(lane->fork, s);
+        cudaStreamWaitEvent(lane->s, lane->fork, 0);
+        ds = lane->s;
     }
-    return n;
+    if (dl) {  // launched first, so its blocks start beside the sweep's first wave
+        if (p.on) k_dl_cells<T, true><<<cdiv(D.ncell, 128), 128, 0, ds>>>(f, p, D);
+        else k_dl_cells<T, false><<<cdiv(D.ncell, 128), 128, 0, ds>>>(f, p, D);
+    }
+    const int n = sh.by == 4 ? e_tma_by<T, 4>(M, f, p, D, G, sh.kc, err, s) : e_tma_by<T, 8>(M, f, p, D, G, sh.kc, err, s);
+    if (beside) {
+        cudaEventRecord(lane->join, lane->s);
+        cudaStreamWaitEvent(s, lane->join, 0);
+    }
+    return n + (dl ? 1 : 0);
 }
 
 template <typename T>
@@ -249,8 +260,10 @@ template int launch_h_tma<float>(const TmaMaps &, const FieldView<float> &, cons
 template int launch_h_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &, FusedShape,
                                    int *, cudaStream_t);
 template int launch_e_tma<float>(const TmaMaps &, const FieldView<float> &, const PmlView<float> &,
-                                  const DlView<float> &, const GainView<float> &, FusedShape, int *, cudaStream_t);
+                                  const DlView<float> &, const GainView<float> &, FusedShape, int *, cudaStream_t,
+                                  const SideLane *);
 template int launch_e_tma<double>(const TmaMaps &, const FieldView<double> &, const PmlView<double> &,
-                                   const DlView<double> &, const GainView<double> &, FusedShape, int *, cudaStream_t);
+                                   const DlView<double> &, const GainView<double> &, FusedShape, int *, cudaStream_t,
+                                   const SideLane *);
 
 }  // namespace cps
