@@ -98,8 +98,9 @@ def parse():
                     help="steps of each job timed on the FP64 plain path (scaled to the job's length; 0: skip)")
     ap.add_argument("--serve-tile", default="",
                     help="batch tile of the serving loop as rows,planes,mode (empty: the library default)")
-    ap.add_argument("--serve-load", type=float, default=2.0,
-                    help="offered load: arrival rate x job work / 20 Gcell-upd/s")
+    ap.add_argument("--serve-load", type=float, default=4.0,
+                    help="offered load: arrival rate x job work / 20 Gcell-upd/s (4: about twice what the "
+                         "server completes, so the GPU stays saturated while jobs arrive)")
     a = ap.parse_args()
     if a.n == 0:
         a.n = 384 if a.workload == "laser" else 256
