@@ -89,8 +89,10 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="time steps in the CPU baseline sample")
     ap.add_argument("--ens-grids", type=int, default=256, help="grids of the batched ensemble leg (0: skip)")
     ap.add_argument("--ens-steps", type=int, default=128, help="timed steps of the batched ensemble")
+    ap.add_argument("--ens-tile", default="",
+                    help="batch tile of the ensemble as rows,planes,mode (empty: autotuned)")
     ap.add_argument("--ens-loop-steps", type=int, default=64,
-                    help="steps per grid of the one-grid-per-launch comparison loops")
+                    help="steps per grid of the one-grid-per-launch comparison loops (0: skip them)")
     ap.add_argument("--serve-jobs", type=int, default=24, help="jobs of the serving leg (0: skip)")
     ap.add_argument("--serve-step-scale", type=float, default=1.0,
                     help="job step counts are the log-uniform [500, 20000] draws divided by this")
@@ -613,7 +615,11 @@ def ensemble(args, local, dist):
     cache = os.path.join(os.path.expanduser("~"), ".cache", "cpsfdtd_b200", "batch_tune.txt")
     os.makedirs(os.path.dirname(cache), exist_ok=True)
     t1 = time.perf_counter()
-    tuned_steps = b.autotune(cache, trial_steps=4)
+    if args.ens_tile:
+        b.set_tile(*(int(v) for v in args.ens_tile.split(",")))
+        tuned_steps = 0
+    else:
+        tuned_steps = b.autotune(cache, trial_steps=4)
     tune_s = time.perf_counter() - t1
     b.step(128)  # warm-up: a direct 64-step chunk, then its graph capture and replay
     b.sync()
@@ -654,14 +660,16 @@ def ensemble(args, local, dist):
         s1.synchronize()
         return cells * steps / (s0.elapsed_time(s1) / 1e3) / 1e9
 
-    loop(cps.FUSED, 2)  # warm-up of the one-grid kernels
-    plain = loop(cps.PLAIN, args.ens_loop_steps)
-    fused = loop(cps.FUSED, args.ens_loop_steps)
+    plain = fused = None
+    if args.ens_loop_steps > 0:
+        loop(cps.FUSED, 2)  # warm-up of the one-grid kernels
+        plain = loop(cps.PLAIN, args.ens_loop_steps)
+        fused = loop(cps.FUSED, args.ens_loop_steps)
     for g in grids:
         g.close()
     # the plain form proper: FP64, one grid per launch (the parity form)
     plain64 = None
-    if not args.no_fp64:
+    if not args.no_fp64 and args.ens_loop_steps > 0:
         g64 = [cps.Grid.from_deck(decks.config4_member(nx, ny, nz, seed=i, steps=5000, nfreq=32), cps.FP64,
                                   device=local) for i, (nx, ny, nz) in enumerate(shapes)]
         loop(cps.PLAIN, 2, g64)
