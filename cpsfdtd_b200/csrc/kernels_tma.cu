@@ -13,10 +13,15 @@ namespace {
 
 // One block per tile of the launch's boxes.  PM selects the body: 0 the
 // CPML-free body for every tile, 1 the CPML body for every tile, 2 the body
-// each tile needs (tile_in_pml).  A sweep with gain launches its CPML tiles
-// (PM 1) and interior tiles (PM 0) separately, so the interior blocks are not
-// held to the CPML body's register count; other sweeps run one launch (PM 2),
-// where a second launch's extra partial wave would cost more than it saves.
+// each tile needs (tile_in_pml).  Sweeps without gain run one launch (PM 2).
+// An FP32 sweep with gain (its gain words staged with the fields) runs every
+// tile on the CPML body in one launch (PM 1; the body leaves cells outside
+// the slabs as the CPML-free body would, bit for bit): measured faster than
+// CPML and interior tiles as two launches at every grid size tried, 128^3 to
+// 384^3, since a second launch's partial last wave costs more than the
+// interior blocks gain from the CPML-free body's lower register count.  An
+// FP64 sweep with gain (gain words read on the cell list) keeps the two
+// launches, so its interior blocks are not held to the CPML body's registers.
 template <typename T, int BY, int PM, bool DL, bool GAIN>
 __global__ void __launch_bounds__(32 * BY, GAIN ? 512 / (32 * BY) : 1024 / (32 * BY))
     k_e_tma(const __grid_constant__ TmaMaps M, FieldView<T> f, PmlView<T> p, DlView<T> D, GainView<T> G, int kc,
@@ -191,6 +196,11 @@ int e_tma_by(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, const
 {
     const bool dl = D.on && D.ncell > 0, gn = G.on && G.ncell > 0;
     const SweepTiles t = sweep_tiles(p.np, p.on, f.d, BY, kc, true);
+    if (gn && sizeof(T) == 4 && p.on) {  // every tile on the CPML body, one launch
+        const TileBoxes all = whole_grid(f.d, BY, kc);
+        return dl ? e_tma_launch<T, BY, 1, true, true>(M, f, p, D, G, kc, all, err, s)
+                  : e_tma_launch<T, BY, 1, false, true>(M, f, p, D, G, kc, all, err, s);
+    }
     if (gn) {  // CPML tiles (if any) and interior tiles as two launches
         return (dl ? e_tma_launch<T, BY, 1, true, true>(M, f, p, D, G, kc, t.pml, err, s)
                    : e_tma_launch<T, BY, 1, false, true>(M, f, p, D, G, kc, t.pml, err, s)) +
