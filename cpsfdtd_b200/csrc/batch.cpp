@@ -88,6 +88,7 @@ struct cps_batch {
     // configuration
     int by = 4, kc = 16, persistent = 2, graph = 1;  // per-member launches: fastest on the measured mixes
     int kch = 0;  // planes per tile of the per-member H sweeps (0: kc)
+    int kcg = 0;  // planes per tile of the per-member FP32 E sweeps with gain (0: kc)
     // device tables (owned)
     std::vector<void *> owned;
     void *d_grids = nullptr;
@@ -411,7 +412,7 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         per_member(b, [&](int gi, cudaStream_t ms) {
             const cps_grid *g = b->grids[gi];
             n += launch_e_tma<T>(g->tma, field_view<T>(g), pml_view<T>(g), dl_view<T>(g), gain_view<T>(g),
-                            FusedShape{b->by, b->kc}, b->d_err, ms, &g->lane);
+                            FusedShape{b->by, b->kc, 0, b->kcg}, b->d_err, ms, &g->lane);
         });
         launch_inject_batch<T>(G, b->d_inj[0], b->ninj[0], 0, s, st);
         launch_sources_batch<T>(G, b->d_src, b->nsrc, s, st);
@@ -546,11 +547,12 @@ bool cache_lookup(const char *path, const std::string &key, int *by, int *kc, in
 
 }  // namespace
 
-void cps::batch_set_h_planes(cps_batch *b, int kch)
+void cps::batch_set_h_planes(cps_batch *b, int kch, int kcg)
 {
-    if (b->kch != kch) {
+    if (b->kch != kch || b->kcg != kcg) {
         b->kch = kch;
-        b->dirty = true;  // captured chunks launch the per-member H sweeps with it
+        b->kcg = kcg;
+        b->dirty = true;  // captured chunks launch the per-member sweeps with them
     }
 }
 

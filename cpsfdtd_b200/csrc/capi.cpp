@@ -1573,7 +1573,7 @@ cps_status solo_step(cps_grid *g, int32_t nsteps)
     if ((rows != g->shape.by || planes != g->shape.kc || pers != 0) &&
         (s = cps_batch_set_tile(g->solo, g->shape.by, g->shape.kc, 0)))
         return s;
-    batch_set_h_planes(g->solo, g->shape.kch);
+    batch_set_h_planes(g->solo, g->shape.kch, g->shape.kcg);
     int64_t l0 = 0, l1 = 0;
     cps_batch_launch_count(g->solo, &l0);
     s = cps_batch_step(g->solo, nsteps);
@@ -2164,6 +2164,7 @@ extern "C" cps_status cps_grid_set_tile(cps_grid *g, int32_t rows, int32_t plane
     g->shape.by = rows;
     g->shape.kc = planes;
     g->shape.kch = planes;
+    g->shape.kcg = planes;
     return CPS_OK;
 }
 

@@ -269,6 +269,7 @@ struct FusedShape {
     int by;       // rows per block (block = 32 x by threads)
     int kc;       // planes per block along z (E sweep; H sweep too when kch is 0)
     int kch = 0;  // planes per block of the TMA H sweep (0: kc)
+    int kcg = 0;  // planes per block of an FP32 TMA E sweep with gain (0: kc)
 };
 // A second stream of a grid with a fork and a join event: work that does not
 // depend on a sweep (the Drude-Lorentz cell pass beside the E sweep) runs on

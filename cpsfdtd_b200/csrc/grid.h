@@ -152,7 +152,7 @@ struct cps_grid {
     int64_t launches = 0;
     // the E sweep's tiles march 8 planes, the H sweep's 16 (measured fastest
     // on the laser and dispersive decks); cps_grid_set_tile sets both
-    FusedShape shape{4, 8, 16};
+    FusedShape shape{4, 8, 16, 4};
     double *d_conv = nullptr;
     unsigned long long *d_counter = nullptr;
     // TMA tensor maps of the fused sweeps (built for tile rows tma_by)
@@ -345,7 +345,8 @@ inline ThreeView three_view(const cps_grid *g)
 
 // clears the device error word of a batch (batch.cpp)
 cps_status batch_clear_error(cps_batch *b);
-// planes per tile of the H sweeps a batch launches per member (0: its kc)
-void batch_set_h_planes(cps_batch *b, int kch);
+// planes per tile of the H sweeps and of the FP32 E sweeps with gain that a
+// batch launches per member (0: its kc)
+void batch_set_h_planes(cps_batch *b, int kch, int kcg = 0);
 
 }  // namespace cps
