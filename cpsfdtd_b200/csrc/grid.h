@@ -150,8 +150,9 @@ struct cps_grid {
     // misc
     int64_t step = 1;
     int64_t launches = 0;
-    // the E sweep's tiles march 8 planes, the H sweep's 16 (measured fastest
-    // on the laser and dispersive decks); cps_grid_set_tile sets both
+    // the E sweep's tiles march 8 planes, the H sweep's 16 and an FP32 E
+    // sweep with gain 4 (measured fastest on the laser and dispersive decks);
+    // cps_grid_set_tile sets all three
     FusedShape shape{4, 8, 16, 4};
     double *d_conv = nullptr;
     unsigned long long *d_counter = nullptr;

@@ -248,10 +248,10 @@ int launch_e_tma(const TmaMaps &M, const FieldView<T> &f, const PmlView<T> &p, c
         if (p.on) k_dl_cells<T, true><<<cdiv(D.ncell, 128), 128, 0, ds>>>(f, p, D);
         else k_dl_cells<T, false><<<cdiv(D.ncell, 128), 128, 0, ds>>>(f, p, D);
     }
-    // an FP32 sweep with gain takes its own plane count (4 by default: its
-    // three-stage ring of large stages measured 1.9 % faster on 4-plane tiles
-    // than on 8 on the 384^3 laser deck, where the E sweep without gain is 9 %
-    // slower on 4 than on 8 on the 256^3 dispersive deck)
+    // an FP32 sweep with gain takes its own plane count (4 by default: with
+    // its three-stage ring of large stages it ran 1.9 % faster on 4-plane
+    // tiles than on 8 on the 384^3 laser deck, while the E sweep without gain
+    // ran 9 % slower on 4 than on 8 on the 256^3 dispersive deck)
     const int kc = G.on && G.ncell > 0 && sizeof(T) == 4 && sh.kcg > 0 ? sh.kcg : sh.kc;
     const int n = sh.by == 4 ? e_tma_by<T, 4>(M, f, p, D, G, kc, err, s) : e_tma_by<T, 8>(M, f, p, D, G, kc, err, s);
     if (beside) {

@@ -248,7 +248,7 @@ __device__ __forceinline__ bool e_tma_body(const TmaMaps &M, const FieldView<T> 
             gain_warp(G, d, j, k, t.bx, act, id, ex, ey, ez);
         }
         // ID-2 cells are left untouched here: the Drude-Lorentz cell kernel
-        // updates them (ADE, then CPML) after the sweep, in the reference order
+        // updates them (ADE, then CPML, the reference order) beside the sweep
         if (act && !(DL && id == CPS_ID_DISPERSIVE)) {
             if (PML) pml_e_cell_pre(p, d, pc, pml_ce_cell(p, f.bE, id), i, j, k, qc, dHz_i, dHy_i, dHx_j, dHz_j, dHy_k, dHx_k, ex, ey, ez);
             const int64_t g = d.idx(i, j, k);
