@@ -111,11 +111,6 @@ struct cps_batch {
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> side_done;
     cudaEvent_t fork = nullptr;
-    // the contraction of a chunk's first ring slots runs on dft_s beside the
-    // chunk's last steps (fork after the gather that fills them, join before
-    // the contraction of the remaining slots)
-    cudaStream_t dft_s = nullptr;
-    cudaEvent_t dft_fork = nullptr, dft_join = nullptr;
     // graphs per chunk length
     std::map<int, std::pair<cudaGraphExec_t, int64_t>> graphs;  // executable and its kernel count
     std::map<int, int> direct;  // chunk lengths launched directly since the last rebuild
@@ -372,11 +367,6 @@ cps_status rebuild_T(cps_batch *b)
         }
     }
     if ((s = ensure_side_streams(b))) return s;
-    if (!dft.empty() && !b->dft_s) {  // made here, outside any capture
-        CK(cudaStreamCreateWithFlags(&b->dft_s, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&b->dft_fork, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&b->dft_join, cudaEventDisableTiming));
-    }
     if ((s = upload_vec(b, &b->d_dl, dl))) return s;
     b->ndl = (int)dl.size();
     for (int side = 0; side < 2; ++side) {
@@ -407,10 +397,6 @@ int64_t enqueue_chunk(cps_batch *b, int S)
     const BatchPort<T> *P = (const BatchPort<T> *)b->d_ports;
     cudaStream_t st = b->stream;
     int64_t n = 0;
-    // chunks of 16 steps or more contract their first three quarters of ring
-    // slots on dft_s while the last quarter's steps run (each contraction
-    // reads and writes the accumulators once, so short chunks keep one)
-    const int split = b->ndft > 0 && b->nphasor > 0 && b->dft_s && S >= 16 ? 3 * S / 4 : 0;
     for (int s = 0; s < S; ++s) {
         launch_h_batch<T>(G, b->d_tiles[kHInt], b->ntiles[kHInt], b->nblocks[kHInt], b->by, false, b->d_err, st);
         launch_h_batch<T>(G, b->d_tiles[kHPml], b->ntiles[kHPml], b->nblocks[kHPml], b->by, true, b->d_err, st);
@@ -433,22 +419,9 @@ int64_t enqueue_chunk(cps_batch *b, int S)
         launch_gather_batch<T>(G, P, b->d_gather, b->ngather, s, S - 1, st);
         for (int c = 0; c < kNumSweep; ++c) n += b->ntiles[c] > 0;
         n += (b->ndl > 0) + (b->ninj[0] > 0) + (b->ninj[1] > 0) + (b->nsrc > 0) + (b->ngather > 0);
-        if (split > 0 && s == split - 1) {  // slots [0, split) are filled: contract them beside the next steps
-            cudaEventRecord(b->dft_fork, st);
-            cudaStreamWaitEvent(b->dft_s, b->dft_fork, 0);
-            launch_phasors_batch<T>(G, P, b->d_phasor, b->nphasor, S, b->dft_s);
-            launch_dft_range_batch<T>(P, b->d_dft, b->ndft, 0, split, b->dft_s);
-            cudaEventRecord(b->dft_join, b->dft_s);
-        }
     }
-    if (split > 0) {
-        cudaStreamWaitEvent(st, b->dft_join, 0);
-        launch_dft_range_batch<T>(P, b->d_dft, b->ndft, split, S - split, st);
-        n += 3;
-    } else {
-        launch_dft_batch<T>(G, P, b->d_phasor, b->nphasor, b->d_dft, b->ndft, S, st);
-        n += b->ndft > 0 ? 2 : 0;
-    }
+    launch_dft_batch<T>(G, P, b->d_phasor, b->nphasor, b->d_dft, b->ndft, S, st);
+    n += b->ndft > 0 ? 2 : 0;
     launch_advance_batch<T>((BatchGrid<T> *)b->d_grids, (int)b->grids.size(), S, st);
     return n + 1;
 }
@@ -623,9 +596,6 @@ extern "C" cps_status cps_batch_destroy(cps_batch *b)
     for (cudaStream_t st : b->side) cudaStreamDestroy(st);
     for (cudaEvent_t e : b->side_done) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
-    if (b->dft_fork) cudaEventDestroy(b->dft_fork);
-    if (b->dft_join) cudaEventDestroy(b->dft_join);
-    if (b->dft_s) cudaStreamDestroy(b->dft_s);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return CPS_OK;

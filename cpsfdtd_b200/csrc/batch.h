@@ -91,16 +91,6 @@ void launch_gather_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, c
 template <typename T>
 void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
                       const int4 *blocks, int nblocks, int nslots, cudaStream_t s);
-// the two halves of launch_dft_batch: the chunk's phasor table (nslots slots
-// from each grid's chunk start), and the contraction of ring slots
-// [s0, s0 + nslots); contractions of consecutive slot ranges, in order, add
-// every sample exactly as one contraction of the whole range does
-template <typename T>
-void launch_phasors_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
-                          int nslots, cudaStream_t s);
-template <typename T>
-void launch_dft_range_batch(const BatchPort<T> *ports, const int4 *blocks, int nblocks, int s0, int nslots,
-                            cudaStream_t s);
 // set the shared-memory attributes of every batched kernel (outside captures)
 template <typename T>
 void batch_kernel_attributes();

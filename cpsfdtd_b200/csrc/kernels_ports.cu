@@ -208,19 +208,16 @@ __global__ void k_phasors_batch(const BatchGrid<T> *__restrict__ grids, const Ba
     phasor_entry(P.omega, P.nfreq, kMaxRing, B.n0, B.dt, q, P.tab);
 }
 
-// ring slots [s0, s0 + nslots) of every port with a DFT (their phasors at
-// the same offset of the chunk's table)
 template <typename T>
 __global__ void __launch_bounds__(256, 2) k_dft_batch(const BatchPort<T> *__restrict__ ports,
-                                                   const int4 *__restrict__ blocks, int s0, int nslots)
+                                                   const int4 *__restrict__ blocks, int nslots)
 {
     extern __shared__ __align__(16) unsigned char sh_raw[];
     const int4 e = blocks[blockIdx.x];
     const BatchPort<T> &P = ports[e.x];
     const int comp = P.comps[e.z];
-    const T *ring = P.ring + (int64_t)s0 * 6 * P.npts;
-    const double2 *tab = P.tab + (comp >= 3 ? (int64_t)kMaxRing * P.nfreq : 0) + (int64_t)s0 * P.nfreq;
-    dft_block<T>(ring, P.npts, nslots, tab, P.nfreq, comp, e.z, e.y, e.w, P.acc, sh_raw);
+    dft_block<T>(P.ring, P.npts, nslots, P.tab + (comp >= 3 ? (int64_t)kMaxRing * P.nfreq : 0), P.nfreq, comp, e.z,
+                 e.y, e.w, P.acc, sh_raw);
 }
 
 // flux[f] = 0.5 * Re sum_p (A_p conj(B_p) - C_p conj(D_p)) * dA over the
@@ -320,29 +317,13 @@ bool dft_batch_attributes()
 }
 
 template <typename T>
-void launch_phasors_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
-                          int nslots, cudaStream_t s)
-{
-    if (nph <= 0 || nslots <= 0) return;
-    k_phasors_batch<T><<<nph, 256, 0, s>>>(grids, ports, ph_blocks, nslots);
-}
-
-template <typename T>
-void launch_dft_range_batch(const BatchPort<T> *ports, const int4 *blocks, int nblocks, int s0, int nslots,
-                            cudaStream_t s)
-{
-    if (nblocks <= 0 || nslots <= 0) return;
-    if (!dft_batch_attributes<T>()) return;
-    k_dft_batch<T><<<nblocks, 256, kDftSmem(sizeof(T)), s>>>(ports, blocks, s0, nslots);
-}
-
-template <typename T>
 void launch_dft_batch(const BatchGrid<T> *grids, const BatchPort<T> *ports, const int2 *ph_blocks, int nph,
                       const int4 *blocks, int nblocks, int nslots, cudaStream_t s)
 {
     if (nph <= 0 || nblocks <= 0 || nslots <= 0) return;
-    launch_phasors_batch<T>(grids, ports, ph_blocks, nph, nslots, s);
-    launch_dft_range_batch<T>(ports, blocks, nblocks, 0, nslots, s);
+    k_phasors_batch<T><<<nph, 256, 0, s>>>(grids, ports, ph_blocks, nslots);
+    if (!dft_batch_attributes<T>()) return;
+    k_dft_batch<T><<<nblocks, 256, kDftSmem(sizeof(T)), s>>>(ports, blocks, nslots);
 }
 
 void launch_port_flux(const double *acc, int npts, int nfreq, int ncomp, const int32_t *sel, double dA,
@@ -384,9 +365,6 @@ void launch_from_device_layout(const T *src, double *dst, Dims d, cudaStream_t s
                                          int, cudaStream_t);                                               \
     template void launch_dft_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int,       \
                                       const int4 *, int, int, cudaStream_t);                             \
-    template void launch_phasors_batch<T>(const BatchGrid<T> *, const BatchPort<T> *, const int2 *, int,   \
-                                          int, cudaStream_t);                                              \
-    template void launch_dft_range_batch<T>(const BatchPort<T> *, const int4 *, int, int, int, cudaStream_t); \
     template bool dft_batch_attributes<T>();
 CPS_INST(double)
 CPS_INST(float)
