@@ -378,7 +378,10 @@ CPS_API cps_status cps_ports_flush(cps_grid *g);
  * milliseconds.  stride 0 turns it off and clears the samples. */
 CPS_API cps_status cps_grid_set_timing(cps_grid *g, int32_t stride);
 /* tile of the fused sweeps: rows (4, 8 or 16) of 32 columns per block and
- * planes marched per block (>= 1); the default is 4 rows x 8 planes */
+ * planes marched per block (>= 1), set for every sweep; the default is 4 rows
+ * with 8 planes for the E sweep, 16 for the H sweep and 4 for an FP32 E sweep
+ * with gain.  cps_grid_get_tile returns the rows and the E sweep's planes.
+ * Tiling does not change results. */
 CPS_API cps_status cps_grid_set_tile(cps_grid *g, int32_t rows, int32_t planes);
 CPS_API cps_status cps_grid_get_tile(const cps_grid *g, int32_t *rows, int32_t *planes);
 /* fused sweep kind: 0 (default) stages x-y tiles of several planes in shared
